@@ -1,0 +1,197 @@
+/*
+ * sr_cuda.h — the C ABI of the B200 field update (hydro + FFT gravity + implicit FLD) of sandbox_reactions.
+ *
+ * This is the drop-in boundary for the reference's `sr-engine` step API (Rust over wgpu). Every entry point below names
+ * the reference interface it replaces (paths relative to the reference project). A thin Rust `extern "C"` crate maps
+ * 1:1 onto these functions; Python reaches them through ctypes.
+ *
+ * Conventions (the reference's canonical layout, crates/sr-engine/src/state.rs:1-38):
+ *   - planes are f32, channel-major, row-major inside a plane: value (c, x, y) at c*W*H + y*W + x, y down;
+ *   - channels: 0 Σ (surface density), 1 Σu, 2 Σv, 3 E (energy per area), then species mass fractions when the
+ *     reference EOS carries them (not in this build: `channels` is 4);
+ *   - x faces: (W+1)*H values, face (x, y) between cells (x-1, y) and (x, y); y faces: W*(H+1) values, face (x, y)
+ *     between (x, y-1) and (x, y); a flux is positive toward +x / +y (crates/sr-physics/src/reference/heat.rs:94-101).
+ *
+ * Ownership and threading: a context owns all of its device memory and one CUDA stream; host buffers are borrowed for
+ * the duration of a call only. One host thread per context (the reference's Step is !Sync). No callbacks.
+ *
+ * Errors: every call returns an sr_status. An unconverged implicit solve is a report flag, not an error
+ * (crates/sr-engine/src/step/heat.rs:215-235). sr_last_error() gives the message of the last failed call.
+ */
+#ifndef SR_CUDA_H
+#define SR_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SR_ABI_VERSION 1u
+
+typedef enum sr_status {
+    SR_OK = 0,
+    SR_E_INVALID = 1,   /* refused arguments: the FftError / StateError / TwinError analogue */
+    SR_E_NONFINITE = 2, /* a non-finite value in the state: the CLI's exit 5 (reduce.wgsl guard) */
+    SR_E_TIMEOUT = 3,   /* a bounded device-side wait expired */
+    SR_E_CUDA = 4,      /* a CUDA runtime error */
+    SR_E_NOMEM = 5,     /* device allocation failed */
+    SR_E_UNSUPPORTED = 6
+} sr_status;
+
+/* Edge modes (crates/sr-physics/src/reference/hydro.rs:183-188; scene "edge"). */
+enum { SR_EDGE_BOUNCE = 0, SR_EDGE_LEAVE = 1 };
+/* Slope limiters: the reference's monotonised central (hydro.rs:283-289) and minmod. */
+enum { SR_LIMITER_MC = 0, SR_LIMITER_MINMOD = 1 };
+/* Gravity kernels: the reference's exact self cell K(0,0) = -4 ln(1+sqrt 2) G (reference/grav.rs:25-34), or
+ * Plummer-softened -G / sqrt(r^2 + eps^2). */
+enum { SR_KERNEL_SELF_CELL = 0, SR_KERNEL_SOFTENED = 1 };
+/* Preconditioners of the implicit FLD solve (crates/sr-engine/src/step/heat.rs:137-141), plus the learned one. */
+enum { SR_PRECOND_MG = 0, SR_PRECOND_JACOBI = 1, SR_PRECOND_LEARNED = 2 };
+
+/*
+ * The run's configuration: the world, the scene's switches, the scheme's choices and physics.json's constants
+ * (assets/physics.json; crates/sr-engine/src/step/mod.rs:399-527 takes them as &Physics/&Passes/&HeatSetup).
+ * Fill with sr_config_default() and override fields.
+ */
+typedef struct sr_config {
+    uint32_t struct_size;     /* sizeof(sr_config): guards against a header/library mismatch */
+    uint32_t width, height;   /* multiples of 8, 8..4096 */
+    uint32_t channels;        /* 4: Σ, Σu, Σv, E */
+    uint32_t edge;            /* SR_EDGE_* */
+    uint32_t limiter;         /* SR_LIMITER_* */
+    uint32_t thermal_bracket; /* 1: the reference's HOT_FACE bracket on Σ and Π slopes (hydro.rs:310-331) */
+    uint32_t gravity;         /* switches (reference/mod.rs:46-56) */
+    uint32_t hydro;
+    uint32_t heat;
+    uint32_t kernel;          /* SR_KERNEL_* */
+    uint32_t precond;         /* SR_PRECOND_* */
+    uint32_t flux_limiter;    /* 1: Levermore-Pomraning λ(R); 0: λ = 1/3 (heat.rs TestFlags) */
+    uint32_t opacity_plane;   /* 1: κ per cell from sr_upload_opacity; 0: κ = kappa0 everywhere */
+    uint32_t mg_pre, mg_post; /* red-black sweeps before / after the coarse correction: V(mg_pre, mg_post) */
+    uint32_t max_passes;      /* Newton passes per implicit step (reference heat.rs:51 MAX_PASSES = 128) */
+    uint32_t max_rounds;      /* PCG rounds over all passes (heat.rs:52 MAX_ROUNDS = 4096) */
+    uint32_t pin_temperature; /* heat.rs TestFlags::pin_temperature */
+    uint32_t reserved[4];
+    double gamma;             /* adiabatic index: Π = (γ-1) Σ ε_th, c² = γΠ/Σ (the reference hardwires γ = 2) */
+    double mu;                /* mean molecular weight: T = μ (γ-1) ε_th (the reference's T = μ ε_th at γ = 2) */
+    double t_floor;           /* physics.json t_floor */
+    double sigma_vac;         /* physics.json sigma_vac */
+    double sigma_floor;       /* physics.json sigma_floor */
+    double cfl;               /* physics.json cfl */
+    double eta_g;             /* physics.json eta_g */
+    double G;                 /* gravitational constant (1 in sandbox units) */
+    double softening;         /* ε of SR_KERNEL_SOFTENED, in cells */
+    double a_r;               /* radiation constant */
+    double c_sb;              /* c in the flux law */
+    double kappa0;            /* opacity when no plane is given */
+    double k_cond;            /* conduction coefficient */
+    double chi;               /* > 0: the constant-diffusivity test flag (u = T, D_f = χ C_f) */
+    double solve_tol;         /* FP64 relative residual each Newton pass's linear solve reaches (1e-8) */
+    double newton_heat;       /* Newton stop: Σ C|ΔT| <= newton_heat Σ C T⁰ ... */
+    double newton_cell;       /* ... and every |ΔT| <= newton_cell T */
+    double dt_fixed;          /* > 0: every step runs on this Δt instead of the CFL/gravity one */
+    double dt_cap;            /* > 0: Δt_{n+1} = min(Δt_{n+1}, dt_cap) (reference/mod.rs:213-216) */
+    double reserved_d[4];
+} sr_config;
+
+/* Δt record (crates/sr-engine/src/step/dt.rs:51-61). */
+typedef struct sr_dt_report {
+    double dt;          /* Δt_n of the last step run */
+    double dt_next;     /* Δt_{n+1} */
+    uint64_t steps;     /* steps run since the context was made */
+    double sim_time;    /* Σ Δt in step order, f64 */
+    int32_t non_finite; /* 1 when the guard found a non-finite value */
+    int32_t nf_channel; /* its channel */
+    int64_t nf_cell;    /* its cell index y*W+x */
+} sr_dt_report;
+
+/* Implicit-step report (crates/sr-engine/src/step/heat.rs:215-235, reference/heat.rs:106-124). */
+typedef struct sr_heat_report {
+    double dt;            /* Δt the step covered; 0 when P5 did not run */
+    uint32_t passes;      /* Newton passes */
+    uint32_t rounds;      /* preconditioned CG rounds over all passes */
+    uint32_t refinements; /* FP64 outer refinement sweeps over all passes */
+    uint32_t converged;   /* 0: ceiling reached, committed by limited fluxes */
+    double delta;         /* heat-balance closure δ */
+    double radiated;      /* heat lost to vacuum and through the edges */
+    double rel_residual;  /* FP64 ||b - A u|| / ||b|| of the last pass's solve */
+    uint32_t fallback_used; /* 1: the learned preconditioner stalled and plain MG-PCG finished the solve */
+    uint32_t precond;       /* SR_PRECOND_* that finished the last solve */
+} sr_heat_report;
+
+/* Per-pass device time of the last sr_step call with timing on (crates/sr-engine/src/step/mod.rs:171-350). */
+typedef struct sr_cost {
+    uint32_t steps;
+    uint32_t pad;
+    double gravity_ms;   /* P2 */
+    double hydro_ms;     /* P4, its mid-step gravity solve included */
+    double heat_ms;      /* P5 */
+    double floors_ms;    /* P8 */
+    double dt_ms;        /* P9 */
+    double total_ms;
+    double hydro_update_ms; /* the fused hydro update kernel alone (the roofline kernel) */
+    uint32_t hydro_update_launches;
+    uint32_t pad2;
+} sr_cost;
+
+/* Fills `cfg` with physics.json's shipped constants and the reference's scheme (MC, bounce, γ = 2, self-cell kernel). */
+void sr_config_default(sr_config* cfg);
+
+/* Returns SR_ABI_VERSION. */
+uint32_t sr_abi_version(void);
+
+typedef struct sr_ctx sr_ctx;
+
+/* Step::with_heat / with_passes / with_neutrino_heating (crates/sr-engine/src/step/mod.rs:399-527): validates `cfg`
+ * (World 8..4096 per axis, multiple of 8; the reference's WorldConfig::validate, state.rs:72-90) and allocates every
+ * buffer of the step on the current device. */
+sr_status sr_create(const sr_config* cfg, sr_ctx** out);
+void sr_destroy(sr_ctx* ctx);
+
+/* State::upload (crates/sr-engine/src/state.rs:251): `nplanes` canonical f32 planes. Resets the step count and the
+ * clock, solves P2 on the state and reduces Δt_0 from it (reference/mod.rs:129-177, Twin::new). */
+sr_status sr_upload(sr_ctx* ctx, const float* planes, uint32_t nplanes);
+/* State::readback (state.rs:273). */
+sr_status sr_readback(sr_ctx* ctx, float* planes, uint32_t nplanes);
+/* The opacity plane κ (W*H f32) read when cfg.opacity_plane is 1. */
+sr_status sr_upload_opacity(sr_ctx* ctx, const float* kappa);
+
+/* Step::run (step/mod.rs:703-718): `steps` steps in the reference's order P1 → P2 → P4 → P5 → P8 → P9
+ * (reference/mod.rs:264-297). Returns SR_E_NONFINITE when the guard finds a non-finite value. */
+sr_status sr_step(sr_ctx* ctx, uint32_t steps);
+
+/* Step::read_dt (step/dt.rs:173). */
+sr_status sr_read_dt(sr_ctx* ctx, sr_dt_report* out);
+/* Step::read_heat (step/heat.rs:499-512). */
+sr_status sr_read_heat(sr_ctx* ctx, sr_heat_report* out);
+/* Step::gravity_field (step/mod.rs:532-534): P2's field of the state the last step started from; W*H each. */
+sr_status sr_gravity_field(sr_ctx* ctx, float* gx, float* gy, float* phi);
+/* Step::read_heat_flux (step/heat.rs:542-548): the last implicit step's solved face fluxes, (W+1)*H and W*(H+1). */
+sr_status sr_heat_flux(sr_ctx* ctx, float* fx, float* fy);
+
+/* Step::set_edge_mode (step/mod.rs:544-548). */
+sr_status sr_set_edge_mode(sr_ctx* ctx, uint32_t edge);
+/* Step::set_heat_precond (step/heat.rs:595-599). */
+sr_status sr_set_heat_precond(sr_ctx* ctx, uint32_t precond);
+/* Step::set_heat_rounds (step/heat.rs:529-533): the ceilings of the implicit step. */
+sr_status sr_set_heat_limits(sr_ctx* ctx, uint32_t max_passes, uint32_t max_rounds);
+/* Step::set_timing / read_cost (step/mod.rs:722-777). */
+sr_status sr_set_timing(sr_ctx* ctx, int32_t on);
+sr_status sr_read_cost(sr_ctx* ctx, sr_cost* out);
+
+/* The first Newton pass's linear system of one implicit step on the uploaded state, solved alone to cfg.solve_tol
+ * with `precond` — the reference's heat_first_system / apply_heat_precond test hooks (step/heat.rs:609-672).
+ * `ms` gets the device time of the solve, `rounds` its preconditioned CG rounds; `x` (optional, W*H f64) the solution. */
+sr_status sr_heat_first_solve(sr_ctx* ctx, double dt, uint32_t precond, double* ms, uint32_t* rounds,
+                              double* rel_residual, double* x);
+
+/* The message of the last failed call on `ctx` (or of the last failed sr_create when ctx is NULL). */
+const char* sr_last_error(const sr_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SR_CUDA_H */
