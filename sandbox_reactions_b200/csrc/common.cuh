@@ -1,0 +1,113 @@
+// common.cuh — shared device/host helpers of the B200 field update: error plumbing, the scheme's parameters and the
+// per-cell physics of the config-mode EOS (Π = (γ-1)Σε, c² = γΠ/Σ, T = μ(γ-1)ε), in FP32.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/sr_cuda.h"
+
+#define SR_HOST_DEVICE __host__ __device__ __forceinline__
+
+// ------------------------------------------------------------------------------------------------ error plumbing
+struct SrError {
+    sr_status status;
+    std::string message;
+};
+
+#define SR_CUDA_TRY(expr)                                                                                     \
+    do {                                                                                                      \
+        cudaError_t e_ = (expr);                                                                              \
+        if (e_ != cudaSuccess)                                                                                \
+            throw SrError{e_ == cudaErrorMemoryAllocation ? SR_E_NOMEM : SR_E_CUDA,                           \
+                          std::string(#expr) + ": " + cudaGetErrorString(e_)};                               \
+    } while (0)
+
+#define SR_REQUIRE(cond, msg)                                      \
+    do {                                                           \
+        if (!(cond)) throw SrError{SR_E_INVALID, std::string(msg)}; \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------------ scheme constants
+// The hydro scheme's scalars, passed by value to every hydro kernel.
+struct HydroConst {
+    int w, h;
+    int edge, limiter, bracket;
+    float gamma, gm1, eps_floor, sigma_vac, sigma_floor;
+};
+
+struct Prim {
+    float s, u, v, p;  // Σ, u, v, Π
+};
+
+struct Face {
+    float U[4];  // conserved Σ, Σu, Σv, E
+    Prim p;      // the primitives it stands for
+};
+
+SR_HOST_DEVICE float eos_pi(const HydroConst& H, float s, float eps) { return H.gm1 * s * eps; }
+
+// A cell as primitives (reference hydro.rs:424-441): the floor state below Σ_vac, else ε_th floored at T_floor/(μ(γ-1)).
+SR_HOST_DEVICE Prim eos_read(const HydroConst& H, float s, float mx, float my, float E) {
+    Prim p;
+    if (s < H.sigma_vac) {
+        p.s = H.sigma_floor;
+        p.u = 0.0f;
+        p.v = 0.0f;
+        p.p = eos_pi(H, H.sigma_floor, H.eps_floor);
+        return p;
+    }
+    float kinetic = 0.5f * (mx * mx + my * my) / (s * s);
+    float raw = E / s - kinetic;
+    float eps = raw < H.eps_floor ? H.eps_floor : raw;
+    p.s = s;
+    p.u = mx / s;
+    p.v = my / s;
+    p.p = eos_pi(H, s, eps);
+    return p;
+}
+
+// The conserved vector of primitives (hydro.rs:443-460).
+SR_HOST_DEVICE void eos_cons(const HydroConst& H, const Prim& p, float* U) {
+    float thermal = p.p / p.s / H.gm1;
+    float eps = fmaxf(thermal, H.eps_floor);
+    U[0] = p.s;
+    U[1] = p.s * p.u;
+    U[2] = p.s * p.v;
+    U[3] = p.s * eps + 0.5f * p.s * (p.u * p.u + p.v * p.v);
+}
+
+// The primitives of a conserved vector, false when it is no state (hydro.rs:462-478).
+SR_HOST_DEVICE bool eos_prim(const HydroConst& H, const float* U, Prim& out) {
+    float s = U[0];
+    if (!(s > 0.0f)) return false;  // NaN or <= 0
+    if (!(isfinite(U[0]) && isfinite(U[1]) && isfinite(U[2]) && isfinite(U[3]))) return false;
+    float raw = U[3] / s - 0.5f * (U[1] * U[1] + U[2] * U[2]) / (s * s);
+    if (!(raw > 0.0f)) return false;
+    float eps = fmaxf(raw, H.eps_floor);
+    out.s = s;
+    out.u = U[1] / s;
+    out.v = U[2] / s;
+    out.p = eos_pi(H, s, eps);
+    return true;
+}
+
+SR_HOST_DEVICE float eos_sound(const HydroConst& H, const Prim& p) {
+    float c2 = H.gamma * p.p / p.s;
+    return sqrtf(fmaxf(c2, 0.0f));
+}
+
+// The Euler flux through a face normal to `dir` (hydro.rs:485-499).
+SR_HOST_DEVICE void euler_flux(const Prim& p, float energy, int dir, float* f) {
+    float un = dir == 0 ? p.u : p.v, ut = dir == 0 ? p.v : p.u;
+    float mass = p.s * un;
+    f[0] = mass;
+    f[1 + dir] = mass * un + p.p;
+    f[2 - dir] = mass * ut;
+    f[3] = (energy + p.p) * un;
+}
+
+// ------------------------------------------------------------------------------------------------ launch helpers
+static inline unsigned div_up(unsigned a, unsigned b) { return (a + b - 1) / b; }

@@ -1,0 +1,469 @@
+// ctx.cu — the C ABI (include/sr_cuda.h): one context per world, owning its device buffers and one stream, and the
+// step driver that runs the reference's pass order P1 → P2 → P4 → P5 → P8 → P9 (reference/mod.rs:264-297) as kernel
+// launches on that stream. Δt lives on the device (the P9 → P1 hand-off never visits the host); the host reads back
+// only at the end of sr_step (the non-finite guard) and in the report calls.
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "grav.cuh"
+#include "heat.cuh"
+#include "hydro.cuh"
+
+namespace {
+thread_local std::string g_create_error;
+}
+
+struct sr_ctx {
+    sr_config cfg{};
+    HydroConst H{};
+    int w = 0, h = 0;
+    size_t n = 0;
+    cudaStream_t stream = nullptr;
+    float* U[2] = {nullptr, nullptr};
+    int cur = 0;
+    float *phi = nullptr, *gx = nullptr, *gy = nullptr;             // P2's field of the step's start state
+    float *src = nullptr, *phim = nullptr, *gxm = nullptr, *gym = nullptr;  // the half step's source and field
+    float* kappa = nullptr;
+    GravPlan grav;
+    bool grav_ready = false;
+    double* part_d = nullptr;
+    float* part_best = nullptr;
+    int* part_idx = nullptr;
+    double* hreport = nullptr;  // 7 doubles
+    DtRecord* rec = nullptr;
+    float *part_rate = nullptr, *part_g = nullptr;
+    long long* part_nf = nullptr;
+    HeatSolver* heat = nullptr;
+    sr_heat_report heat_report{};
+    bool uploaded = false;
+    // timing
+    bool timing = false;
+    std::vector<cudaEvent_t> events;
+    sr_cost cost{};
+    std::string error;
+};
+
+static void validate(const sr_config& c) {
+    SR_REQUIRE(c.struct_size == sizeof(sr_config), "sr_config.struct_size does not match this library's sr_config");
+    SR_REQUIRE(c.width >= 16 && c.width <= 4096 && c.width % 8 == 0,
+               "world width must be a multiple of 8 in 16..4096 (got " + std::to_string(c.width) + ")");
+    SR_REQUIRE(c.height >= 16 && c.height <= 4096 && c.height % 8 == 0,
+               "world height must be a multiple of 8 in 16..4096 (got " + std::to_string(c.height) + ")");
+    SR_REQUIRE(c.channels == 4, "this build carries 4 channels (Σ, Σu, Σv, E)");
+    SR_REQUIRE(c.edge <= SR_EDGE_LEAVE, "unknown edge mode");
+    SR_REQUIRE(c.limiter <= SR_LIMITER_MINMOD, "unknown limiter");
+    SR_REQUIRE(c.kernel <= SR_KERNEL_SOFTENED, "unknown gravity kernel");
+    SR_REQUIRE(c.precond <= SR_PRECOND_LEARNED, "unknown preconditioner");
+    SR_REQUIRE(c.gamma > 1.0, "gamma must exceed 1");
+    SR_REQUIRE(c.mu > 0.0, "mu must be positive");
+    SR_REQUIRE(c.t_floor > 0.0, "t_floor must be positive");
+    SR_REQUIRE(c.sigma_vac > 0.0 && c.sigma_floor > 0.0, "sigma_vac and sigma_floor must be positive");
+    SR_REQUIRE(c.cfl > 0.0 && c.eta_g > 0.0, "cfl and eta_g must be positive");
+    SR_REQUIRE(!(c.kernel == SR_KERNEL_SOFTENED && !(c.softening > 0.0)), "the softened kernel needs softening > 0");
+    SR_REQUIRE(c.dt_fixed >= 0.0 && c.dt_cap >= 0.0, "dt_fixed and dt_cap must be >= 0");
+}
+
+static HydroConst hydro_const(const sr_config& c) {
+    HydroConst H;
+    H.w = (int)c.width;
+    H.h = (int)c.height;
+    H.edge = (int)c.edge;
+    H.limiter = (int)c.limiter;
+    H.bracket = (int)c.thermal_bracket;
+    H.gamma = (float)c.gamma;
+    H.gm1 = (float)(c.gamma - 1.0);
+    H.eps_floor = (float)(c.t_floor / c.mu / (c.gamma - 1.0));
+    H.sigma_vac = (float)c.sigma_vac;
+    H.sigma_floor = (float)c.sigma_floor;
+    return H;
+}
+
+template <class T>
+static void dalloc(T** p, size_t count) {
+    SR_CUDA_TRY(cudaMalloc((void**)p, sizeof(T) * (count ? count : 1)));
+    SR_CUDA_TRY(cudaMemset(*p, 0, sizeof(T) * (count ? count : 1)));
+}
+
+static void ctx_free(sr_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->U[0]);
+    cudaFree(c->U[1]);
+    cudaFree(c->phi); cudaFree(c->gx); cudaFree(c->gy);
+    cudaFree(c->src); cudaFree(c->phim); cudaFree(c->gxm); cudaFree(c->gym);
+    cudaFree(c->kappa);
+    if (c->grav_ready) c->grav.destroy();
+    cudaFree(c->part_d); cudaFree(c->part_best); cudaFree(c->part_idx); cudaFree(c->hreport);
+    cudaFree(c->rec); cudaFree(c->part_rate); cudaFree(c->part_g); cudaFree(c->part_nf);
+    if (c->heat) heat_destroy(c->heat);
+    for (auto e : c->events) cudaEventDestroy(e);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+// Runs `body`, turning an SrError or a CUDA error into a status and the context's message.
+template <class F>
+static sr_status guarded(sr_ctx* c, F body) {
+    if (!c) return SR_E_INVALID;
+    try {
+        body();
+        return SR_OK;
+    } catch (const SrError& e) {
+        c->error = e.message;
+        return e.status;
+    } catch (const std::exception& e) {
+        c->error = e.what();
+        return SR_E_CUDA;
+    }
+}
+
+static float* planes(sr_ctx* c) { return c->U[c->cur]; }
+
+// P2 on the current state, then P9 (no floors) — what Twin::new does before step 0 (reference/mod.rs:129-177).
+static void initial_reductions(sr_ctx* c) {
+    DtRecord rec{};
+    SR_CUDA_TRY(cudaMemcpyAsync(c->rec, &rec, sizeof rec, cudaMemcpyHostToDevice, c->stream));
+    SR_CUDA_TRY(cudaMemsetAsync(c->hreport, 0, 7 * sizeof(double), c->stream));
+    if (c->cfg.gravity) c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
+    const sr_config& k = c->cfg;
+    floors_dt_launch(c->H, planes(c), k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 0, c->part_rate,
+                     c->part_g, c->part_nf, k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec, c->stream);
+    SR_CUDA_TRY(cudaGetLastError());
+}
+
+static cudaEvent_t event_at(sr_ctx* c, size_t i) {
+    while (c->events.size() <= i) {
+        cudaEvent_t e;
+        SR_CUDA_TRY(cudaEventCreate(&e));
+        c->events.push_back(e);
+    }
+    return c->events[i];
+}
+
+static HydroArgs hydro_args(sr_ctx* c) {
+    HydroArgs A{};
+    A.H = c->H;
+    A.dt = &c->rec->dt;
+    A.U = c->U[c->cur];
+    A.Uout = c->U[1 - c->cur];
+    A.gx = c->cfg.gravity ? c->gx : nullptr;
+    A.gy = c->cfg.gravity ? c->gy : nullptr;
+    A.src = c->src;
+    A.phim = c->phim;
+    A.gxm = c->gxm;
+    A.gym = c->gym;
+    A.part_d = c->part_d;
+    A.part_best = c->part_best;
+    A.part_idx = c->part_idx;
+    A.report = c->hreport;
+    return A;
+}
+
+static void run_steps(sr_ctx* c, uint32_t steps) {
+    const sr_config& k = c->cfg;
+    // event slots per step: 0 start, 1 after P2, 2 hydro update start, 3 hydro update end, 4 after P4, 5 after P5,
+    // 6 after P8/P9
+    const int E = 7;
+    for (uint32_t s = 0; s < steps; s++) {
+        auto mark = [&](int slot) {
+            if (c->timing) SR_CUDA_TRY(cudaEventRecord(event_at(c, (size_t)s * E + slot), c->stream));
+        };
+        mark(0);
+        dt_advance_launch(c->rec, c->stream);
+        if (k.gravity) c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
+        mark(1);
+        if (k.hydro) {
+            HydroArgs A = hydro_args(c);
+            if (k.gravity) {
+                hydro_launch(kHydroSource, A, c->stream);
+                c->grav.solve(c->src, c->phim, c->gxm, c->gym, c->stream);
+                mark(2);
+                hydro_launch(kHydroUpdateGrav, A, c->stream);
+                mark(3);
+                hydro_finalize_launch(A, 1, c->stream);
+            } else {
+                mark(2);
+                hydro_launch(kHydroUpdate, A, c->stream);
+                mark(3);
+                hydro_finalize_launch(A, 0, c->stream);
+            }
+            c->cur = 1 - c->cur;
+        } else {
+            mark(2);
+            mark(3);
+        }
+        mark(4);
+        if (k.heat) heat_step(c->heat, planes(c), k.opacity_plane ? c->kappa : nullptr, &c->rec->dt, c->stream,
+                              &c->heat_report);
+        mark(5);
+        floors_dt_launch(c->H, planes(c), k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 1, c->part_rate,
+                         c->part_g, c->part_nf, k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec, c->stream);
+        mark(6);
+        SR_CUDA_TRY(cudaGetLastError());
+    }
+    if (c->timing && steps) {
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        sr_cost& t = c->cost;
+        memset(&t, 0, sizeof t);
+        t.steps = steps;
+        for (uint32_t s = 0; s < steps; s++) {
+            float ms[6];
+            for (int q = 0; q < 6; q++) {
+                int a = q, b = q + 1;
+                SR_CUDA_TRY(cudaEventElapsedTime(&ms[q], c->events[(size_t)s * E + a], c->events[(size_t)s * E + b]));
+            }
+            t.gravity_ms += ms[0];
+            t.hydro_ms += ms[1] + ms[2] + ms[3];
+            t.hydro_update_ms += ms[2];
+            t.heat_ms += ms[4];
+            t.dt_ms += ms[5];
+            float total;
+            SR_CUDA_TRY(cudaEventElapsedTime(&total, c->events[(size_t)s * E], c->events[(size_t)s * E + 6]));
+            t.total_ms += total;
+        }
+        t.hydro_update_launches = k.hydro ? steps : 0;
+    }
+}
+
+extern "C" {
+
+void sr_config_default(sr_config* c) {
+    memset(c, 0, sizeof *c);
+    c->struct_size = sizeof(sr_config);
+    c->width = 64;
+    c->height = 64;
+    c->channels = 4;
+    c->edge = SR_EDGE_BOUNCE;
+    c->limiter = SR_LIMITER_MC;
+    c->thermal_bracket = 1;
+    c->hydro = 1;
+    c->kernel = SR_KERNEL_SELF_CELL;
+    c->precond = SR_PRECOND_MG;
+    c->flux_limiter = 1;
+    c->mg_pre = 2;
+    c->mg_post = 2;
+    c->max_passes = 128;
+    c->max_rounds = 4096;
+    c->gamma = 2.0;
+    c->mu = 1.0;
+    c->t_floor = 0.05;
+    c->sigma_vac = 1e-6;
+    c->sigma_floor = 1e-8;
+    c->cfl = 0.4;
+    c->eta_g = 0.3;
+    c->G = 1.0;
+    c->softening = 1.0;
+    c->a_r = 6.25e-7;
+    c->c_sb = 12800.0;
+    c->kappa0 = 1.0;
+    c->k_cond = 0.0;
+    c->chi = 0.0;
+    c->solve_tol = 1e-8;
+    c->newton_heat = 1e-9;
+    c->newton_cell = 1e-7;
+}
+
+uint32_t sr_abi_version(void) { return SR_ABI_VERSION; }
+
+sr_status sr_create(const sr_config* cfg, sr_ctx** out) {
+    if (!cfg || !out) {
+        g_create_error = "sr_create: null argument";
+        return SR_E_INVALID;
+    }
+    *out = nullptr;
+    sr_ctx* c = new sr_ctx();
+    try {
+        validate(*cfg);
+        c->cfg = *cfg;
+        c->H = hydro_const(*cfg);
+        c->w = (int)cfg->width;
+        c->h = (int)cfg->height;
+        c->n = (size_t)c->w * c->h;
+        const size_t n = c->n;
+        SR_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        dalloc(&c->U[0], 4 * n);
+        dalloc(&c->U[1], 4 * n);
+        dalloc(&c->phi, n);
+        dalloc(&c->gx, n);
+        dalloc(&c->gy, n);
+        if (cfg->gravity) {
+            dalloc(&c->src, n);
+            dalloc(&c->phim, n);
+            dalloc(&c->gxm, n);
+            dalloc(&c->gym, n);
+            c->grav.create(c->w, c->h, (int)cfg->kernel, cfg->G, cfg->softening, (float)cfg->sigma_vac);
+            c->grav_ready = true;
+        }
+        if (cfg->opacity_plane) dalloc(&c->kappa, n);
+        int hb = hydro_blocks(c->w, c->h);
+        dalloc(&c->part_d, (size_t)hb * 6);
+        dalloc(&c->part_best, (size_t)hb);
+        dalloc(&c->part_idx, (size_t)hb);
+        dalloc(&c->hreport, 7);
+        dalloc(&c->rec, 1);
+        int fb = floors_dt_blocks(c->w, c->h);
+        dalloc(&c->part_rate, (size_t)fb);
+        dalloc(&c->part_g, (size_t)fb);
+        dalloc(&c->part_nf, (size_t)fb);
+        if (cfg->heat) c->heat = heat_create(*cfg, c->stream);
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    } catch (const SrError& e) {
+        g_create_error = e.message;
+        ctx_free(c);
+        return e.status;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
+        ctx_free(c);
+        return SR_E_CUDA;
+    }
+    *out = c;
+    return SR_OK;
+}
+
+void sr_destroy(sr_ctx* ctx) { ctx_free(ctx); }
+
+sr_status sr_upload(sr_ctx* c, const float* p, uint32_t nplanes) {
+    return guarded(c, [&] {
+        SR_REQUIRE(p, "sr_upload: null planes");
+        SR_REQUIRE(nplanes == 4, "sr_upload: this build carries 4 planes");
+        SR_CUDA_TRY(cudaMemcpyAsync(planes(c), p, sizeof(float) * 4 * c->n, cudaMemcpyHostToDevice, c->stream));
+        initial_reductions(c);
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        c->uploaded = true;
+    });
+}
+
+sr_status sr_readback(sr_ctx* c, float* p, uint32_t nplanes) {
+    return guarded(c, [&] {
+        SR_REQUIRE(p, "sr_readback: null planes");
+        SR_REQUIRE(nplanes == 4, "sr_readback: this build carries 4 planes");
+        SR_CUDA_TRY(cudaMemcpyAsync(p, planes(c), sizeof(float) * 4 * c->n, cudaMemcpyDeviceToHost, c->stream));
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+}
+
+sr_status sr_upload_opacity(sr_ctx* c, const float* kappa) {
+    return guarded(c, [&] {
+        SR_REQUIRE(kappa, "sr_upload_opacity: null plane");
+        SR_REQUIRE(c->cfg.opacity_plane, "sr_upload_opacity: the context was made without opacity_plane");
+        SR_CUDA_TRY(cudaMemcpyAsync(c->kappa, kappa, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+}
+
+sr_status sr_step(sr_ctx* c, uint32_t steps) {
+    sr_status st = guarded(c, [&] {
+        SR_REQUIRE(c->uploaded, "sr_step: no state uploaded");
+        run_steps(c, steps);
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+    if (st != SR_OK) return st;
+    DtRecord rec;
+    st = guarded(c, [&] { SR_CUDA_TRY(cudaMemcpy(&rec, c->rec, sizeof rec, cudaMemcpyDeviceToHost)); });
+    if (st != SR_OK) return st;
+    if (rec.non_finite) {
+        c->error = "non-finite value at cell " + std::to_string(rec.nf_cell) + " channel " +
+                   std::to_string(rec.nf_channel) + " after step " + std::to_string(rec.nf_step);
+        return SR_E_NONFINITE;
+    }
+    return SR_OK;
+}
+
+sr_status sr_read_dt(sr_ctx* c, sr_dt_report* out) {
+    return guarded(c, [&] {
+        SR_REQUIRE(out, "sr_read_dt: null report");
+        DtRecord rec;
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        SR_CUDA_TRY(cudaMemcpy(&rec, c->rec, sizeof rec, cudaMemcpyDeviceToHost));
+        out->dt = rec.dt;
+        out->dt_next = rec.dt_next;
+        out->steps = rec.steps;
+        out->sim_time = rec.sim_time;
+        out->non_finite = rec.non_finite;
+        out->nf_channel = rec.nf_channel;
+        out->nf_cell = rec.nf_cell;
+    });
+}
+
+sr_status sr_read_heat(sr_ctx* c, sr_heat_report* out) {
+    return guarded(c, [&] {
+        SR_REQUIRE(out, "sr_read_heat: null report");
+        SR_REQUIRE(c->cfg.heat, "sr_read_heat: the context runs no heat pass");
+        *out = c->heat_report;
+    });
+}
+
+sr_status sr_gravity_field(sr_ctx* c, float* gx, float* gy, float* phi) {
+    return guarded(c, [&] {
+        SR_REQUIRE(c->cfg.gravity, "sr_gravity_field: the context runs no gravity pass");
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (gx) SR_CUDA_TRY(cudaMemcpy(gx, c->gx, sizeof(float) * c->n, cudaMemcpyDeviceToHost));
+        if (gy) SR_CUDA_TRY(cudaMemcpy(gy, c->gy, sizeof(float) * c->n, cudaMemcpyDeviceToHost));
+        if (phi) SR_CUDA_TRY(cudaMemcpy(phi, c->phi, sizeof(float) * c->n, cudaMemcpyDeviceToHost));
+    });
+}
+
+sr_status sr_heat_flux(sr_ctx* c, float* fx, float* fy) {
+    return guarded(c, [&] {
+        SR_REQUIRE(c->cfg.heat, "sr_heat_flux: the context runs no heat pass");
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        heat_read_flux(c->heat, fx, fy);
+    });
+}
+
+sr_status sr_set_edge_mode(sr_ctx* c, uint32_t edge) {
+    return guarded(c, [&] {
+        SR_REQUIRE(edge <= SR_EDGE_LEAVE, "unknown edge mode");
+        c->cfg.edge = edge;
+        c->H.edge = (int)edge;
+    });
+}
+
+sr_status sr_set_heat_precond(sr_ctx* c, uint32_t precond) {
+    return guarded(c, [&] {
+        SR_REQUIRE(precond <= SR_PRECOND_LEARNED, "unknown preconditioner");
+        SR_REQUIRE(c->cfg.heat, "sr_set_heat_precond: the context runs no heat pass");
+        c->cfg.precond = precond;
+        heat_set_precond(c->heat, precond);
+    });
+}
+
+sr_status sr_set_heat_limits(sr_ctx* c, uint32_t max_passes, uint32_t max_rounds) {
+    return guarded(c, [&] {
+        SR_REQUIRE(max_passes >= 1 && max_rounds >= 1, "heat limits must be >= 1");
+        SR_REQUIRE(c->cfg.heat, "sr_set_heat_limits: the context runs no heat pass");
+        c->cfg.max_passes = max_passes;
+        c->cfg.max_rounds = max_rounds;
+        heat_set_limits(c->heat, max_passes, max_rounds);
+    });
+}
+
+sr_status sr_set_timing(sr_ctx* c, int32_t on) {
+    return guarded(c, [&] { c->timing = on != 0; });
+}
+
+sr_status sr_read_cost(sr_ctx* c, sr_cost* out) {
+    return guarded(c, [&] {
+        SR_REQUIRE(out, "sr_read_cost: null report");
+        *out = c->cost;
+    });
+}
+
+sr_status sr_heat_first_solve(sr_ctx* c, double dt, uint32_t precond, double* ms, uint32_t* rounds,
+                              double* rel_residual, double* x) {
+    return guarded(c, [&] {
+        SR_REQUIRE(c->cfg.heat, "sr_heat_first_solve: the context runs no heat pass");
+        SR_REQUIRE(c->uploaded, "sr_heat_first_solve: no state uploaded");
+        SR_REQUIRE(dt > 0.0, "sr_heat_first_solve: dt must be positive");
+        SR_REQUIRE(precond <= SR_PRECOND_LEARNED, "unknown preconditioner");
+        heat_first_solve(c->heat, planes(c), c->cfg.opacity_plane ? c->kappa : nullptr, dt, precond, c->stream, ms,
+                         rounds, rel_residual, x);
+    });
+}
+
+const char* sr_last_error(const sr_ctx* c) { return c ? c->error.c_str() : g_create_error.c_str(); }
+
+}  // extern "C"

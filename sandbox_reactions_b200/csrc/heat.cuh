@@ -1,0 +1,18 @@
+// heat.cuh — P5, the implicit flux-limited diffusion step: Newton passes, each an SPD 5-point system solved by
+// multigrid-preconditioned CG in FP32 inside an FP64 iterative-refinement loop.
+#pragma once
+
+#include "common.cuh"
+
+struct HeatSolver;
+
+HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s);
+void heat_destroy(HeatSolver* hs);
+// One implicit step of length *dt_dev on the 4 planes U (E changes), κ from `kappa` (W*H) or cfg.kappa0.
+void heat_step(HeatSolver* hs, float* U, const float* kappa, const double* dt_dev, cudaStream_t s, sr_heat_report* rep);
+void heat_read_flux(HeatSolver* hs, float* fx, float* fy);
+void heat_set_precond(HeatSolver* hs, uint32_t precond);
+void heat_set_limits(HeatSolver* hs, uint32_t max_passes, uint32_t max_rounds);
+// The first Newton pass's system of a step of length dt, solved alone (timed on the device).
+void heat_first_solve(HeatSolver* hs, const float* U, const float* kappa, double dt, uint32_t precond, cudaStream_t s,
+                      double* ms, uint32_t* rounds, double* rel_residual, double* x);

@@ -1,0 +1,196 @@
+"""Host-side mirror of the reference's `sr-engine` step API over the C ABI (include/sr_cuda.h).
+
+`Step` plays the part of the reference's `Step` + `State` pair (crates/sr-engine/src/step/mod.rs:367-777,
+crates/sr-engine/src/state.rs:139-279): it is built from a world configuration, takes the canonical channel-major f32
+planes by `upload`, advances by `run(steps)` and reports Δt, the implicit step, the gravity field and the flux through
+the same calls. Every call goes through libsrcuda.so; there is no CPU path: when the library cannot be loaded the
+constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from .abi import (PRECOND, EDGE, STATUS_NAMES, Config, sr_config, sr_cost, sr_dt_report, sr_heat_report)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsrcuda.so")
+
+_lib = None
+
+
+class SrError(RuntimeError):
+    """A refused or failed call: the status name and the library's message (the reference's FftError/StateError)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libsrcuda.so (built by `sandbox_reactions_b200.build`); raises when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m sandbox_reactions_b200.build`")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    F = C.POINTER(C.c_float)
+    D = C.POINTER(C.c_double)
+    L.sr_config_default.argtypes = [C.POINTER(sr_config)]
+    L.sr_abi_version.restype = C.c_uint32
+    L.sr_create.argtypes = [C.POINTER(sr_config), C.POINTER(P)]
+    L.sr_destroy.argtypes = [P]
+    L.sr_upload.argtypes = [P, F, C.c_uint32]
+    L.sr_readback.argtypes = [P, F, C.c_uint32]
+    L.sr_upload_opacity.argtypes = [P, F]
+    L.sr_step.argtypes = [P, C.c_uint32]
+    L.sr_read_dt.argtypes = [P, C.POINTER(sr_dt_report)]
+    L.sr_read_heat.argtypes = [P, C.POINTER(sr_heat_report)]
+    L.sr_gravity_field.argtypes = [P, F, F, F]
+    L.sr_heat_flux.argtypes = [P, F, F]
+    L.sr_set_edge_mode.argtypes = [P, C.c_uint32]
+    L.sr_set_heat_precond.argtypes = [P, C.c_uint32]
+    L.sr_set_heat_limits.argtypes = [P, C.c_uint32, C.c_uint32]
+    L.sr_set_timing.argtypes = [P, C.c_int32]
+    L.sr_read_cost.argtypes = [P, C.POINTER(sr_cost)]
+    L.sr_heat_first_solve.argtypes = [P, C.c_double, C.c_uint32, D, C.POINTER(C.c_uint32), D, D]
+    L.sr_last_error.restype = C.c_char_p
+    L.sr_last_error.argtypes = [P]
+    for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_step", "sr_read_dt",
+                 "sr_read_heat", "sr_gravity_field", "sr_heat_flux", "sr_set_edge_mode", "sr_set_heat_precond",
+                 "sr_set_heat_limits", "sr_set_timing", "sr_read_cost", "sr_heat_first_solve"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+@dataclass
+class DtReport:
+    dt: float
+    dt_next: float
+    steps: int
+    sim_time: float
+    non_finite: tuple | None
+
+
+class Step:
+    """One world's field update on the GPU (the reference's Step over its State)."""
+
+    def __init__(self, config: Config):
+        self.lib = load_library()
+        self.config = config
+        self._c = config.to_c()
+        h = C.c_void_p()
+        st = self.lib.sr_create(C.byref(self._c), C.byref(h))
+        if st:
+            raise SrError(st, self.lib.sr_last_error(None).decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.sr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int):
+        if st:
+            raise SrError(st, self.lib.sr_last_error(self._h).decode())
+
+    @property
+    def shape(self):
+        return (4, self.config.height, self.config.width)
+
+    # ---- State::upload / readback (state.rs:251-279)
+    def upload(self, planes: np.ndarray):
+        p = np.ascontiguousarray(planes, dtype=np.float32)
+        if p.shape != self.shape:
+            raise SrError(1, f"planes of shape {p.shape}, expected {self.shape}")
+        self._check(self.lib.sr_upload(self._h, _fptr(p), 4))
+
+    def upload_opacity(self, kappa: np.ndarray):
+        k = np.ascontiguousarray(kappa, dtype=np.float32)
+        if k.shape != self.shape[1:]:
+            raise SrError(1, f"opacity plane of shape {k.shape}, expected {self.shape[1:]}")
+        self._check(self.lib.sr_upload_opacity(self._h, _fptr(k)))
+
+    def readback(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float32)
+        self._check(self.lib.sr_readback(self._h, _fptr(out), 4))
+        return out
+
+    # ---- Step::run (step/mod.rs:703-718)
+    def run(self, steps: int = 1):
+        self._check(self.lib.sr_step(self._h, int(steps)))
+
+    # ---- reports
+    def read_dt(self) -> DtReport:
+        r = sr_dt_report()
+        self._check(self.lib.sr_read_dt(self._h, C.byref(r)))
+        nf = (int(r.nf_cell), int(r.nf_channel)) if r.non_finite else None
+        return DtReport(r.dt, r.dt_next, int(r.steps), r.sim_time, nf)
+
+    def read_heat(self) -> sr_heat_report:
+        r = sr_heat_report()
+        self._check(self.lib.sr_read_heat(self._h, C.byref(r)))
+        return r
+
+    def gravity_field(self):
+        h, w = self.shape[1:]
+        gx, gy, phi = (np.empty((h, w), np.float32) for _ in range(3))
+        self._check(self.lib.sr_gravity_field(self._h, _fptr(gx), _fptr(gy), _fptr(phi)))
+        return phi, gx, gy
+
+    def read_heat_flux(self):
+        h, w = self.shape[1:]
+        fx, fy = np.empty((h, w + 1), np.float32), np.empty((h + 1, w), np.float32)
+        self._check(self.lib.sr_heat_flux(self._h, _fptr(fx), _fptr(fy)))
+        return fx, fy
+
+    # ---- switches
+    def set_edge_mode(self, edge: str):
+        self._check(self.lib.sr_set_edge_mode(self._h, EDGE[edge]))
+
+    def set_heat_precond(self, precond: str):
+        self._check(self.lib.sr_set_heat_precond(self._h, PRECOND[precond]))
+
+    def set_heat_limits(self, max_passes: int, max_rounds: int):
+        self._check(self.lib.sr_set_heat_limits(self._h, max_passes, max_rounds))
+
+    def set_timing(self, on: bool = True):
+        self._check(self.lib.sr_set_timing(self._h, int(on)))
+
+    def read_cost(self) -> sr_cost:
+        r = sr_cost()
+        self._check(self.lib.sr_read_cost(self._h, C.byref(r)))
+        return r
+
+    def heat_first_solve(self, dt: float, precond: str = "mg", want_x: bool = False):
+        """The first Newton pass's system solved alone: (device ms, rounds, FP64 rel residual, x or None)."""
+        ms, rel = C.c_double(), C.c_double()
+        rounds = C.c_uint32()
+        h, w = self.shape[1:]
+        x = np.empty((h, w), np.float64) if want_x else None
+        xp = x.ctypes.data_as(C.POINTER(C.c_double)) if want_x else None
+        self._check(self.lib.sr_heat_first_solve(self._h, dt, PRECOND[precond], C.byref(ms), C.byref(rounds),
+                                                 C.byref(rel), xp))
+        return ms.value, rounds.value, rel.value, x
