@@ -1,17 +1,833 @@
-// heat.cu — P5 (placeholder until the FLD solver lands).
-#include "heat.cuh"
+// heat.cu — P5, the implicit flux-limited radiative diffusion step (crates/sr-physics/src/reference/heat.rs:453-592).
+//
+// One backward-Euler step in the heat potential u = a_r T⁴ with the Levermore–Pomraning law frozen at the pass start.
+// Newton passes linearise T(u); each pass is one SPD 5-point system A u = b, solved here by iterative refinement:
+// the residual r = b - A x and the update x += s e in FP64 (s the residual's rms scale), the correction from an FP32
+// preconditioned CG on A e = r/s with FP64 dot products, preconditioned by the FP32 multigrid V-cycle (mg.cu) or
+// Jacobi. The passes stop by the reference's two rules (the heat moved, the largest cell change); the commit closes the
+// heat balance with δ (heat.rs:521-536), or past the ceiling commits by limited fluxes (heat.rs:545-592).
+#include <math.h>
+#include <string.h>
 
-struct HeatSolver {
-    int dummy;
+#include <algorithm>
+#include <vector>
+
+#include "heat.cuh"
+#include "mg.cuh"
+
+namespace {
+
+constexpr int RED_THREADS = 256;
+constexpr int MAX_PART = 4096;
+enum Slot { S_NGAS, S_DT, S_HEAT0, S_RR, S_BB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1, S_MOVED, S_VIOL, S_RAD, S_GAIN, S_HELD, S_COUNT };
+
+struct HeatConst {
+    int w, h;
+    double gm1, mu, t_floor, sigma_vac, sigma_floor, a_r, c_sb, kappa0, k_cond, chi;
+    int limiter_on;
 };
 
-HeatSolver* heat_create(const sr_config&, cudaStream_t) {
-    throw SrError{SR_E_UNSUPPORTED, "the heat pass is not built yet"};
+__device__ __forceinline__ double u_of(const HeatConst& K, double t) {
+    return K.chi > 0.0 ? t : K.a_r * ((t * t) * (t * t));
 }
-void heat_destroy(HeatSolver* hs) { delete hs; }
-void heat_step(HeatSolver*, float*, const float*, const double*, cudaStream_t, sr_heat_report*) {}
-void heat_read_flux(HeatSolver*, float*, float*) {}
-void heat_set_precond(HeatSolver*, uint32_t) {}
-void heat_set_limits(HeatSolver*, uint32_t, uint32_t) {}
-void heat_first_solve(HeatSolver*, const float*, const float*, double, uint32_t, cudaStream_t, double*, uint32_t*,
-                      double*, double*) {}
+__device__ __forceinline__ double t_of(const HeatConst& K, double u) {
+    return K.chi > 0.0 ? u : sqrt(sqrt(u / K.a_r));
+}
+__device__ __forceinline__ double dt_du(const HeatConst& K, double t) {
+    return K.chi > 0.0 ? 1.0 : 1.0 / (4.0 * K.a_r * ((t * t) * t));
+}
+
+// Block reduction of a double into part[blockIdx.x] (fixed order).
+__device__ __forceinline__ void block_sum(double v, double* part) {
+    __shared__ double red[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += red[q];
+        part[blockIdx.x] = t;
+    }
+    __syncthreads();
+}
+
+__global__ void finalize_kernel(const double* __restrict__ part, int count, double* out) {
+    __shared__ double sd[RED_THREADS];
+    const int tid = threadIdx.x;
+    const int per = (count + RED_THREADS - 1) / RED_THREADS;
+    double acc = 0.0;
+    for (int b = tid * per; b < min(count, (tid + 1) * per); b++) acc += part[b];
+    sd[tid] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int k = 0; k < RED_THREADS; k++) t += sd[k];
+        *out = t;
+    }
+}
+
+// ---- step set-up: the sides (heat.rs:215-226), the faces' D_f (heat.rs:263-294), Σ_f k and its vacuum part
+__global__ void heat_cells_kernel(HeatConst K, const float* __restrict__ U, const float* __restrict__ kappa,
+                                  uint8_t* gas, double* t0, double* C, float* kap, float* sig, double* t, double* u,
+                                  double* part, double* part_gas) {
+    const size_t n = (size_t)K.w * K.h;
+    double acc = 0.0, ngas = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double s = U[i];
+        const float k = kappa ? kappa[i] : (float)K.kappa0;
+        kap[i] = k;
+        if (s < K.sigma_vac) {
+            gas[i] = 0;
+            t0[i] = K.t_floor;
+            sig[i] = (float)K.sigma_floor;
+            C[i] = K.sigma_floor / (K.mu * K.gm1);
+            t[i] = K.t_floor;
+            u[i] = u_of(K, K.t_floor);
+            continue;
+        }
+        const double mx = U[n + i], my = U[2 * n + i], e = U[3 * n + i];
+        const double kinetic = 0.5 * (mx * mx + my * my) / (s * s);
+        const double raw = e / s - kinetic;
+        const double floor = K.t_floor / K.mu / K.gm1;
+        const double eps = raw < floor ? floor : raw;
+        const double T = K.mu * K.gm1 * eps;
+        gas[i] = 1;
+        t0[i] = T;
+        sig[i] = (float)s;
+        C[i] = s / (K.mu * K.gm1);
+        t[i] = T;
+        u[i] = u_of(K, T);
+        acc += C[i] * T;
+        ngas += 1.0;
+    }
+    block_sum(acc, part);
+    block_sum(ngas, part_gas);
+}
+
+struct Side {
+    bool gas;
+    double t, s, kappa, c;
+};
+
+__device__ __forceinline__ Side side_at(const HeatConst& K, const uint8_t* gas, const double* t0, const float* kap,
+                                        const float* sig, const double* C, size_t i) {
+    Side o;
+    o.gas = gas[i];
+    o.t = t0[i];
+    o.s = sig[i];
+    o.kappa = kap[i];
+    o.c = C[i];
+    return o;
+}
+
+__device__ __forceinline__ Side vacuum_beyond(const HeatConst& K, const Side& g) {
+    Side o;
+    o.gas = false;
+    o.t = K.t_floor;
+    o.s = K.sigma_floor;
+    o.kappa = g.kappa;
+    o.c = K.sigma_floor / (K.mu * K.gm1);
+    return o;
+}
+
+__device__ __forceinline__ double diffusivity(const HeatConst& K, const Side& a, const Side& b) {
+    if (!a.gas && !b.gas) return 0.0;
+    if (K.chi > 0.0) return K.chi * (0.5 * (a.c + b.c));
+    const double ta2 = a.t * a.t, tb2 = b.t * b.t;
+    const double era = K.a_r * (ta2 * ta2), erb = K.a_r * (tb2 * tb2);
+    const double face_er = 0.5 * (era + erb);
+    const double ks = 0.5 * (a.kappa * a.s + b.kappa * b.s);
+    const double r = face_er > 0.0 ? fabs(erb - era) / (ks * face_er) : 0.0;
+    const double lam = K.limiter_on ? (2.0 + r) / (6.0 + 3.0 * r + r * r) : 1.0 / 3.0;
+    const double radiative = K.c_sb * lam / ks;
+    const double conduction =
+        K.k_cond != 0.0 ? K.k_cond / (K.a_r * (a.t + b.t) * (a.t * a.t + b.t * b.t)) : 0.0;
+    return radiative + conduction;
+}
+
+__device__ __forceinline__ double face_coef(const HeatConst& K, const Side* a, const Side* b) {
+    Side A, B;
+    if (a && b) {
+        if (a->gas || b->gas) {
+            A = a->gas ? *a : vacuum_beyond(K, *b);
+            B = b->gas ? *b : vacuum_beyond(K, *a);
+        } else {
+            A = *a;
+            B = *a;
+        }
+    } else if (a) {
+        A = *a;
+        B = vacuum_beyond(K, *a);
+    } else {
+        A = vacuum_beyond(K, *b);
+        B = *b;
+    }
+    return diffusivity(K, A, B);
+}
+
+__global__ void heat_faces_kernel(HeatConst K, const uint8_t* __restrict__ gas, const double* __restrict__ t0,
+                                  const float* __restrict__ kap, const float* __restrict__ sig,
+                                  const double* __restrict__ C, double* kx, double* ky) {
+    const int w = K.w, h = K.h;
+    const size_t nx = (size_t)(w + 1) * h, ny = (size_t)w * (h + 1);
+    for (size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x; f < nx + ny; f += (size_t)gridDim.x * blockDim.x) {
+        Side a, b;
+        bool ha, hb;
+        if (f < nx) {
+            const int x = (int)(f % (w + 1)), y = (int)(f / (w + 1));
+            ha = x > 0;
+            hb = x < w;
+            if (ha) a = side_at(K, gas, t0, kap, sig, C, (size_t)y * w + x - 1);
+            if (hb) b = side_at(K, gas, t0, kap, sig, C, (size_t)y * w + x);
+            kx[f] = face_coef(K, ha ? &a : nullptr, hb ? &b : nullptr);
+        } else {
+            const size_t g = f - nx;
+            const int x = (int)(g % w), y = (int)(g / w);
+            ha = y > 0;
+            hb = y < h;
+            if (ha) a = side_at(K, gas, t0, kap, sig, C, (size_t)(y - 1) * w + x);
+            if (hb) b = side_at(K, gas, t0, kap, sig, C, (size_t)y * w + x);
+            ky[g] = face_coef(K, ha ? &a : nullptr, hb ? &b : nullptr);
+        }
+    }
+}
+
+__global__ void heat_ksum_kernel(HeatConst K, const uint8_t* __restrict__ gas, const double* __restrict__ kx,
+                                 const double* __restrict__ ky, double* ksum, double* kvac) {
+    const int w = K.w, h = K.h;
+    const size_t n = (size_t)w * h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) {
+            ksum[i] = 0.0;
+            kvac[i] = 0.0;
+            continue;
+        }
+        const int x = (int)(i % w), y = (int)(i / w);
+        const double k[4] = {kx[(size_t)y * (w + 1) + x], kx[(size_t)y * (w + 1) + x + 1], ky[(size_t)y * w + x],
+                             ky[(size_t)(y + 1) * w + x]};
+        const bool nb[4] = {x > 0 && gas[i - 1], x + 1 < w && gas[i + 1], y > 0 && gas[i - w],
+                            y + 1 < h && gas[i + w]};
+        double s = 0.0, v = 0.0;
+        for (int f = 0; f < 4; f++) {
+            s += k[f];
+            if (!nb[f]) v += k[f];
+        }
+        ksum[i] = s;
+        kvac[i] = v;
+    }
+}
+
+// ---- a Newton pass's system at the iterate (heat.rs:476-489) and level 0's excess c = c_i + Σ_vac D_f (FP32)
+__global__ void heat_system_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+                                   const double* __restrict__ C, const double* __restrict__ t,
+                                   const double* __restrict__ u, const double* __restrict__ t0,
+                                   const double* __restrict__ ksum, const double* __restrict__ kvac, double* diag,
+                                   double* rhs, float* c0, double* x) {
+    const size_t n = (size_t)K.w * K.h;
+    const double u_vac = u_of(K, K.t_floor);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) {
+            diag[i] = 1.0;
+            rhs[i] = 0.0;
+            c0[i] = 1.0f;
+            x[i] = 0.0;
+            continue;
+        }
+        const double heat = C[i] / dt;
+        const double ci = heat * dt_du(K, t[i]);
+        diag[i] = ci + ksum[i];
+        rhs[i] = ci * u[i] - heat * (t[i] - t0[i]) + kvac[i] * u_vac;
+        c0[i] = (float)(ci + kvac[i]);
+        x[i] = u[i];
+    }
+}
+
+// r = b - A x in FP64 with partials of <r, r> and <b, b>.
+__global__ void heat_residual64_kernel(HeatConst K, const uint8_t* __restrict__ gas, const double* __restrict__ diag,
+                                       const double* __restrict__ rhs, const double* __restrict__ kx,
+                                       const double* __restrict__ ky, const double* __restrict__ x, double* r,
+                                       double* part_rr, double* part_bb) {
+    const int w = K.w, h = K.h;
+    const size_t n = (size_t)w * h;
+    double rr = 0.0, bb = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) {
+            r[i] = 0.0;
+            continue;
+        }
+        const int xx = (int)(i % w), y = (int)(i / w);
+        double s = diag[i] * x[i];
+        if (xx > 0 && gas[i - 1]) s -= kx[(size_t)y * (w + 1) + xx] * x[i - 1];
+        if (xx + 1 < w && gas[i + 1]) s -= kx[(size_t)y * (w + 1) + xx + 1] * x[i + 1];
+        if (y > 0 && gas[i - w]) s -= ky[(size_t)y * w + xx] * x[i - w];
+        if (y + 1 < h && gas[i + w]) s -= ky[(size_t)(y + 1) * w + xx] * x[i + w];
+        const double ri = rhs[i] - s;
+        r[i] = ri;
+        rr += ri * ri;
+        bb += rhs[i] * rhs[i];
+    }
+    block_sum(rr, part_rr);
+    block_sum(bb, part_bb);
+}
+
+__global__ void scale_kernel(size_t n, const double* __restrict__ r64, double inv_scale, float* r32, float* e32,
+                             double* part) {
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = (float)(r64[i] * inv_scale);
+        r32[i] = v;
+        e32[i] = 0.0f;
+        acc += (double)v * v;
+    }
+    block_sum(acc, part);
+}
+
+// q = A p on level 0's FP32 operator (diagonal c + Σ couplings), partials of <p, q>.
+__global__ void spmv_kernel(MgLevel L, const float* __restrict__ p, float* q, double* part) {
+    const int w = L.w, h = L.h;
+    const size_t n = (size_t)w * h;
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % w), y = (int)(i / w);
+        float v = 0.0f;
+        if (L.mask[i]) {
+            const float dl = x > 0 ? L.dx[i - 1] : 0.0f, du = y > 0 ? L.dy[i - w] : 0.0f;
+            const float dr = L.dx[i], dd = L.dy[i];
+            v = (L.c[i] + dl + dr + du + dd) * p[i];
+            if (x > 0) v -= dl * p[i - 1];
+            if (x + 1 < w) v -= dr * p[i + 1];
+            if (y > 0) v -= du * p[i - w];
+            if (y + 1 < h) v -= dd * p[i + w];
+        }
+        q[i] = v;
+        acc += (double)p[i] * v;
+    }
+    block_sum(acc, part);
+}
+
+// e += α p, r -= α q (α = <r,z>/<p,q> from the device scalars), partials of <r, r>.
+__global__ void pcg_update_kernel(size_t n, const double* __restrict__ scal, int rz_slot, const float* __restrict__ p,
+                                  const float* __restrict__ q, float* e, float* r, double* part) {
+    const float alpha = (float)(scal[rz_slot] / scal[S_PQ]);
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        e[i] += alpha * p[i];
+        const float ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        acc += (double)ri * ri;
+    }
+    block_sum(acc, part);
+}
+
+// p = z + β p (β = <r,z>_new / <r,z>_old); the first direction (old slot < 0) is p = z.
+__global__ void pcg_direction_kernel(size_t n, const double* __restrict__ scal, int old_slot, int new_slot,
+                                     const float* __restrict__ z, float* p) {
+    const float beta = old_slot < 0 ? 0.0f : (float)(scal[new_slot] / scal[old_slot]);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = old_slot < 0 ? z[i] : z[i] + beta * p[i];
+}
+
+// z = r / diag (Jacobi), partials of <r, z>.
+__global__ void jacobi_kernel(MgLevel L, const float* __restrict__ r, float* z, double* part) {
+    const int w = L.w, h = L.h;
+    const size_t n = (size_t)w * h;
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % w), y = (int)(i / w);
+        const float dl = x > 0 ? L.dx[i - 1] : 0.0f, du = y > 0 ? L.dy[i - w] : 0.0f;
+        const float zi = L.mask[i] ? r[i] / (L.c[i] + dl + L.dx[i] + du + L.dy[i]) : 0.0f;
+        z[i] = zi;
+        acc += (double)r[i] * zi;
+    }
+    block_sum(acc, part);
+}
+
+__global__ void correction_kernel(size_t n, const uint8_t* __restrict__ gas, const float* __restrict__ e,
+                                  double scale, double* x) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (gas[i]) x[i] += scale * (double)e[i];
+}
+
+// The pass's update (heat.rs:494-509): u >= u_vac, T within a factor 2; partials of Σ C|ΔT| and of the cells moved
+// by more than newton_cell of their T.
+__global__ void newton_update_kernel(HeatConst K, double cell_tol, const uint8_t* __restrict__ gas,
+                                     const double* __restrict__ C, const double* __restrict__ x, double* t, double* u,
+                                     double* part_moved, double* part_viol) {
+    const size_t n = (size_t)K.w * K.h;
+    const double u_vac = u_of(K, K.t_floor);
+    double moved = 0.0, viol = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) continue;
+        const double ti = t[i];
+        double nx = t_of(K, fmax(x[i], u_vac));
+        nx = fmin(fmax(nx, 0.5 * ti), 2.0 * ti);
+        const double d = fabs(nx - ti);
+        moved += C[i] * d;
+        if (!(d <= cell_tol * ti)) viol += 1.0;
+        t[i] = nx;
+        u[i] = u_of(K, nx);
+    }
+    block_sum(moved, part_moved);
+    block_sum(viol, part_viol);
+}
+
+// F = -k (v_b - v_a) at every face (heat.rs:338-361), v = u on gas cells, u_vac elsewhere; FP32 out.
+__device__ __forceinline__ double face_flux(const HeatConst& K, const uint8_t* gas, const double* u, double k,
+                                            long a, long b, double u_vac) {
+    if (k == 0.0) return 0.0;
+    const double va = (a >= 0 && gas[a]) ? u[a] : u_vac;
+    const double vb = (b >= 0 && gas[b]) ? u[b] : u_vac;
+    return -k * (vb - va);
+}
+
+__global__ void heat_flux_kernel(HeatConst K, const uint8_t* __restrict__ gas, const double* __restrict__ kx,
+                                 const double* __restrict__ ky, const double* __restrict__ u,
+                                 const double* __restrict__ scale, float* fx, float* fy) {
+    const int w = K.w, h = K.h;
+    const size_t nx = (size_t)(w + 1) * h, ny = (size_t)w * (h + 1);
+    const double u_vac = u_of(K, K.t_floor);
+    for (size_t f = (size_t)blockIdx.x * blockDim.x + threadIdx.x; f < nx + ny; f += (size_t)gridDim.x * blockDim.x) {
+        long a, b;
+        double k;
+        if (f < nx) {
+            const int x = (int)(f % (w + 1)), y = (int)(f / (w + 1));
+            a = x > 0 ? (long)y * w + x - 1 : -1;
+            b = x < w ? (long)y * w + x : -1;
+            k = kx[f];
+        } else {
+            const size_t g = f - nx;
+            const int x = (int)(g % w), y = (int)(g / w);
+            a = y > 0 ? (long)(y - 1) * w + x : -1;
+            b = y < h ? (long)y * w + x : -1;
+            k = ky[g];
+        }
+        double F = face_flux(K, gas, u, k, a, b, u_vac);
+        if (scale) {
+            const long from = F > 0.0 ? a : b;
+            F *= from >= 0 ? scale[from] : 1.0;
+        }
+        if (f < nx) fx[f] = (float)F;
+        else fy[f - nx] = (float)F;
+    }
+}
+
+// The commit's sums (heat.rs:521-531): radiated, gained and held.
+__global__ void commit_sums_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+                                   const double* __restrict__ C, const double* __restrict__ t,
+                                   const double* __restrict__ t0, const double* __restrict__ u,
+                                   const double* __restrict__ kvac, double* p_rad, double* p_gain, double* p_held) {
+    const size_t n = (size_t)K.w * K.h;
+    const double u_vac = u_of(K, K.t_floor);
+    double rad = 0.0, gain = 0.0, held = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) continue;
+        rad += dt * kvac[i] * (u[i] - u_vac);
+        gain += C[i] * (t[i] - t0[i]);
+        held += C[i] * t[i];
+    }
+    block_sum(rad, p_rad);
+    block_sum(gain, p_gain);
+    block_sum(held, p_held);
+}
+
+// E_i += C_i ((1 + δ) T_i - T_i⁰) (heat.rs:532-535).
+__global__ void commit_apply_kernel(HeatConst K, double delta, const uint8_t* __restrict__ gas,
+                                    const double* __restrict__ C, const double* __restrict__ t,
+                                    const double* __restrict__ t0, float* U) {
+    const size_t n = (size_t)K.w * K.h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (gas[i]) U[3 * n + i] = (float)((double)U[3 * n + i] + C[i] * ((1.0 + delta) * t[i] - t0[i]));
+}
+
+// Past the ceiling (heat.rs:545-564): each gas cell's outflow scaled to the heat it holds above its floor.
+__global__ void limited_scale_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+                                     const double* __restrict__ kx, const double* __restrict__ ky,
+                                     const double* __restrict__ u, const double* __restrict__ C,
+                                     const double* __restrict__ t0, double* scale) {
+    const int w = K.w, h = K.h;
+    const size_t n = (size_t)w * h;
+    const double u_vac = u_of(K, K.t_floor);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) {
+            scale[i] = 1.0;
+            continue;
+        }
+        const int x = (int)(i % w), y = (int)(i / w);
+        const long L = x > 0 ? (long)i - 1 : -1, R = x + 1 < w ? (long)i + 1 : -1;
+        const long Uu = y > 0 ? (long)i - w : -1, D = y + 1 < h ? (long)i + w : -1;
+        const double lv[4] = {-face_flux(K, gas, u, kx[(size_t)y * (w + 1) + x], L, (long)i, u_vac),
+                              face_flux(K, gas, u, kx[(size_t)y * (w + 1) + x + 1], (long)i, R, u_vac),
+                              -face_flux(K, gas, u, ky[(size_t)y * w + x], Uu, (long)i, u_vac),
+                              face_flux(K, gas, u, ky[(size_t)(y + 1) * w + x], (long)i, D, u_vac)};
+        double out = 0.0;
+        for (int f = 0; f < 4; f++) out += fmax(lv[f], 0.0);
+        out *= dt;
+        const double held = C[i] * fmax(t0[i] - K.t_floor, 0.0);
+        scale[i] = out > held ? held / out : 1.0;
+    }
+}
+
+// E -= Δt Σ_f F_f with every face's F at the scale of the cell it leaves (heat.rs:565-592); partials of radiated.
+__global__ void limited_apply_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+                                     const double* __restrict__ kx, const double* __restrict__ ky,
+                                     const double* __restrict__ u, const double* __restrict__ scale, float* U,
+                                     double* p_rad) {
+    const int w = K.w, h = K.h;
+    const size_t n = (size_t)w * h;
+    const double u_vac = u_of(K, K.t_floor);
+    double rad = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) continue;
+        const int x = (int)(i % w), y = (int)(i / w);
+        const long nb[4] = {x > 0 ? (long)i - 1 : -1, x + 1 < w ? (long)i + 1 : -1, y > 0 ? (long)i - w : -1,
+                            y + 1 < h ? (long)i + w : -1};
+        double F[4] = {face_flux(K, gas, u, kx[(size_t)y * (w + 1) + x], nb[0], (long)i, u_vac),
+                       face_flux(K, gas, u, kx[(size_t)y * (w + 1) + x + 1], (long)i, nb[1], u_vac),
+                       face_flux(K, gas, u, ky[(size_t)y * w + x], nb[2], (long)i, u_vac),
+                       face_flux(K, gas, u, ky[(size_t)(y + 1) * w + x], (long)i, nb[3], u_vac)};
+        // the low cell of faces 0 and 2 is the neighbour, of faces 1 and 3 this cell
+        const long low[4] = {nb[0], (long)i, nb[2], (long)i}, high[4] = {(long)i, nb[1], (long)i, nb[3]};
+        double out[4];
+        for (int f = 0; f < 4; f++) {
+            const long from = F[f] > 0.0 ? low[f] : high[f];
+            F[f] *= from >= 0 ? scale[from] : 1.0;
+        }
+        out[0] = -F[0];
+        out[1] = F[1];
+        out[2] = -F[2];
+        out[3] = F[3];
+        for (int f = 0; f < 4; f++)
+            if (!(nb[f] >= 0 && gas[nb[f]])) rad += dt * out[f];
+        U[3 * n + i] = (float)((double)U[3 * n + i] - dt * (((out[0] + out[1]) + out[2]) + out[3]));
+    }
+    block_sum(rad, p_rad);
+}
+
+int grid_for(size_t n) {
+    size_t b = (n + RED_THREADS - 1) / RED_THREADS;
+    return (int)(b < 1 ? 1 : (b > (size_t)MAX_PART ? (size_t)MAX_PART : b));
+}
+
+}  // namespace
+
+struct HeatSolver {
+    sr_config cfg{};
+    HeatConst K{};
+    int w = 0, h = 0;
+    size_t n = 0;
+    int grid = 0;
+    uint32_t precond = SR_PRECOND_MG;
+    uint32_t max_passes = 128, max_rounds = 4096;
+    double inner_floor = 1e-5;  // the smallest residual reduction asked of one inner FP32 solve
+    uint8_t* gas = nullptr;
+    double *t0 = nullptr, *C = nullptr, *t = nullptr, *u = nullptr, *kx = nullptr, *ky = nullptr;
+    double *ksum = nullptr, *kvac = nullptr, *diag = nullptr, *rhs = nullptr, *x = nullptr, *r64 = nullptr;
+    double* lscale = nullptr;
+    float *kap = nullptr, *sig = nullptr;
+    float *r32 = nullptr, *e32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr;
+    float *fx = nullptr, *fy = nullptr;
+    double* part = nullptr;  // S_COUNT slots of MAX_PART partials
+    double* scal = nullptr;  // S_COUNT device scalars
+    double* hscal = nullptr; // pinned host copy
+    Multigrid mg;
+    int n_gas = 0;
+
+    double* P(int slot) { return part + (size_t)slot * MAX_PART; }
+
+    void finalize(int slot, int count, cudaStream_t s) {
+        finalize_kernel<<<1, RED_THREADS, 0, s>>>(P(slot), count, scal + slot);
+    }
+
+    // Reads device scalars [first, first + count) into hscal (synchronises the stream).
+    void read(int first, int count, cudaStream_t s) {
+        SR_CUDA_TRY(cudaMemcpyAsync(hscal + first, scal + first, sizeof(double) * count, cudaMemcpyDeviceToHost, s));
+        SR_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+};
+
+namespace {
+
+void setup_step(HeatSolver* H, const float* U, const float* kappa, cudaStream_t s) {
+    const HeatConst& K = H->K;
+    heat_cells_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, U, kappa, H->gas, H->t0, H->C, H->kap, H->sig, H->t, H->u,
+                                                      H->P(S_HEAT0), H->P(S_NGAS));
+    H->finalize(S_HEAT0, H->grid, s);
+    H->finalize(S_NGAS, H->grid, s);
+    const size_t nf = (size_t)(H->w + 1) * H->h + (size_t)H->w * (H->h + 1);
+    heat_faces_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(K, H->gas, H->t0, H->kap, H->sig, H->C, H->kx, H->ky);
+    heat_ksum_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, H->gas, H->kx, H->ky, H->ksum, H->kvac);
+    H->mg.set_couplings(H->kx, H->ky, H->gas, s);
+}
+
+// z = M r with partials of <r, z> into slot `rz_slot`.
+void precondition(HeatSolver* H, uint32_t precond, int rz_slot, cudaStream_t s) {
+    if (precond == SR_PRECOND_JACOBI) {
+        jacobi_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, H->P(rz_slot));
+        H->finalize(rz_slot, H->grid, s);
+    } else {
+        H->mg.apply(H->r32, H->z32, s);
+        finalize_kernel<<<1, RED_THREADS, 0, s>>>(H->mg.part, H->mg.part_count, H->scal + rz_slot);
+    }
+}
+
+struct SolveResult {
+    int rounds = 0;
+    int refinements = 0;
+    double rel = 0.0;
+    bool ok = true;
+};
+
+// PCG on A32 e = r32 from e = 0 to a residual reduction `eta` or `max_it` rounds. Returns the rounds, or -1 on a
+// breakdown (a non-positive or non-finite curvature).
+int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStream_t s) {
+    const size_t n = H->n;
+    H->finalize(S_R32, H->grid, s);  // <r, r> of the scaled residual (partials written by scale_kernel)
+    precondition(H, precond, S_RZ0, s);
+    pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, -1, S_RZ0, H->z32, H->p32);
+    H->read(S_R32, 1, s);
+    const double rr0 = H->hscal[S_R32];
+    if (!(rr0 > 0.0)) return 0;
+    int it = 0;
+    int next_check = 1;
+    while (it < max_it) {
+        const int rz_old = (it & 1) ? S_RZ1 : S_RZ0, rz_new = (it & 1) ? S_RZ0 : S_RZ1;
+        spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->P(S_PQ));
+        H->finalize(S_PQ, H->grid, s);
+        pcg_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
+                                                          H->P(S_RRI));
+        H->finalize(S_RRI, H->grid, s);
+        it++;
+        if (it == next_check || it == max_it) {
+            H->read(S_PQ, 2, s);  // S_PQ, S_RRI
+            const double pq = H->hscal[S_PQ], rr = H->hscal[S_RRI];
+            if (!(pq > 0.0) || !isfinite(pq) || !isfinite(rr)) return -1;
+            if (rr <= eta * eta * rr0) break;
+            next_check = it < 4 ? it + 1 : it + 4;
+        }
+        precondition(H, precond, rz_new, s);
+        pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, rz_old, rz_new, H->z32, H->p32);
+    }
+    return it;
+}
+
+// The pass's system to ||b - A x|| <= tol ||b|| by FP64 refinement around FP32 PCG; x starts at the iterate.
+SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_rounds, cudaStream_t s) {
+    SolveResult R;
+    const HeatConst& K = H->K;
+    double prev = INFINITY;
+    for (int ref = 0; ref < 12; ref++) {
+        heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, H->gas, H->diag, H->rhs, H->kx, H->ky, H->x,
+                                                               H->r64, H->P(S_RR), H->P(S_BB));
+        H->finalize(S_RR, H->grid, s);
+        H->finalize(S_BB, H->grid, s);
+        H->read(S_RR, 2, s);
+        const double rr = H->hscal[S_RR], bb = H->hscal[S_BB];
+        if (!isfinite(rr) || !isfinite(bb)) {
+            R.ok = false;
+            return R;
+        }
+        R.rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+        if (R.rel <= tol || rr == 0.0) return R;
+        if (R.rel > 0.5 * prev || R.rounds >= max_rounds) return R;  // stagnating, or out of rounds
+        prev = R.rel;
+        const double scale = sqrt(rr / (double)std::max(1, H->n_gas));
+        scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->P(S_R32));
+        const double eta = std::min(0.5, std::max(H->inner_floor, 0.5 * tol / R.rel));
+        int it = inner_pcg(H, precond, eta, max_rounds - R.rounds, s);
+        if (it < 0) {
+            R.ok = false;
+            return R;
+        }
+        R.rounds += it;
+        R.refinements++;
+        correction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->gas, H->e32, scale, H->x);
+    }
+    return R;
+}
+
+void build_system(HeatSolver* H, double dt, cudaStream_t s) {
+    heat_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->u, H->t0, H->ksum, H->kvac,
+                                                       H->diag, H->rhs, H->mg.L[0].c, H->x);
+    H->mg.coarsen(s);
+}
+
+}  // namespace
+
+HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
+    HeatSolver* H = new HeatSolver();
+    try {
+        H->cfg = cfg;
+        H->w = (int)cfg.width;
+        H->h = (int)cfg.height;
+        H->n = (size_t)H->w * H->h;
+        H->precond = cfg.precond;
+        H->max_passes = cfg.max_passes ? cfg.max_passes : 128;
+        H->max_rounds = cfg.max_rounds ? cfg.max_rounds : 4096;
+        HeatConst& K = H->K;
+        K.w = H->w;
+        K.h = H->h;
+        K.gm1 = cfg.gamma - 1.0;
+        K.mu = cfg.mu;
+        K.t_floor = cfg.t_floor;
+        K.sigma_vac = cfg.sigma_vac;
+        K.sigma_floor = cfg.sigma_floor;
+        K.a_r = cfg.a_r;
+        K.c_sb = cfg.c_sb;
+        K.kappa0 = cfg.kappa0;
+        K.k_cond = cfg.k_cond;
+        K.chi = cfg.chi;
+        K.limiter_on = cfg.flux_limiter != 0;
+        H->grid = grid_for(H->n);
+        const size_t n = H->n, nx = (size_t)(H->w + 1) * H->h, ny = (size_t)H->w * (H->h + 1);
+        SR_CUDA_TRY(cudaMalloc(&H->gas, n));
+        double** d64[] = {&H->t0, &H->C, &H->t, &H->u, &H->ksum, &H->kvac, &H->diag, &H->rhs, &H->x, &H->r64,
+                          &H->lscale};
+        for (double** p : d64) SR_CUDA_TRY(cudaMalloc(p, sizeof(double) * n));
+        SR_CUDA_TRY(cudaMalloc(&H->kx, sizeof(double) * nx));
+        SR_CUDA_TRY(cudaMalloc(&H->ky, sizeof(double) * ny));
+        float** d32[] = {&H->kap, &H->sig, &H->r32, &H->e32, &H->p32, &H->q32, &H->z32};
+        for (float** p : d32) SR_CUDA_TRY(cudaMalloc(p, sizeof(float) * n));
+        SR_CUDA_TRY(cudaMalloc(&H->fx, sizeof(float) * nx));
+        SR_CUDA_TRY(cudaMalloc(&H->fy, sizeof(float) * ny));
+        SR_CUDA_TRY(cudaMemset(H->fx, 0, sizeof(float) * nx));
+        SR_CUDA_TRY(cudaMemset(H->fy, 0, sizeof(float) * ny));
+        SR_CUDA_TRY(cudaMalloc(&H->part, sizeof(double) * MAX_PART * S_COUNT));
+        SR_CUDA_TRY(cudaMalloc(&H->scal, sizeof(double) * S_COUNT));
+        SR_CUDA_TRY(cudaMemset(H->scal, 0, sizeof(double) * S_COUNT));
+        SR_CUDA_TRY(cudaMallocHost(&H->hscal, sizeof(double) * S_COUNT));
+        H->mg.create(H->w, H->h, (int)cfg.mg_pre, (int)cfg.mg_post);
+        (void)s;
+    } catch (...) {
+        heat_destroy(H);
+        throw;
+    }
+    return H;
+}
+
+void heat_destroy(HeatSolver* H) {
+    if (!H) return;
+    cudaFree(H->gas);
+    double* d64[] = {H->t0, H->C, H->t, H->u, H->ksum, H->kvac, H->diag, H->rhs, H->x, H->r64, H->lscale, H->kx, H->ky};
+    for (double* p : d64) cudaFree(p);
+    float* d32[] = {H->kap, H->sig, H->r32, H->e32, H->p32, H->q32, H->z32, H->fx, H->fy};
+    for (float* p : d32) cudaFree(p);
+    cudaFree(H->part);
+    cudaFree(H->scal);
+    if (H->hscal) cudaFreeHost(H->hscal);
+    H->mg.destroy();
+    delete H;
+}
+
+void heat_set_precond(HeatSolver* H, uint32_t precond) {
+    if (precond == SR_PRECOND_LEARNED) throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not loaded"};
+    H->precond = precond;
+}
+
+void heat_set_limits(HeatSolver* H, uint32_t max_passes, uint32_t max_rounds) {
+    H->max_passes = max_passes;
+    H->max_rounds = max_rounds;
+}
+
+void heat_read_flux(HeatSolver* H, float* fx, float* fy) {
+    const size_t nx = (size_t)(H->w + 1) * H->h, ny = (size_t)H->w * (H->h + 1);
+    if (fx) SR_CUDA_TRY(cudaMemcpy(fx, H->fx, sizeof(float) * nx, cudaMemcpyDeviceToHost));
+    if (fy) SR_CUDA_TRY(cudaMemcpy(fy, H->fy, sizeof(float) * ny, cudaMemcpyDeviceToHost));
+}
+
+void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev, cudaStream_t s,
+               sr_heat_report* rep) {
+    sr_heat_report R{};
+    R.precond = H->precond;
+    setup_step(H, U, kappa, s);
+    SR_CUDA_TRY(cudaMemcpyAsync(H->scal + S_DT, dt_dev, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    H->read(S_NGAS, 3, s);  // gas cells, Δt, Σ C T⁰
+    H->n_gas = (int)H->hscal[S_NGAS];
+    const double dt = H->hscal[S_DT];
+    const double heat0 = H->hscal[S_HEAT0];
+    const size_t nf = (size_t)(H->w + 1) * H->h + (size_t)H->w * (H->h + 1);
+    if (H->cfg.pin_temperature || H->n_gas == 0 || !(dt > 0.0)) {
+        heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx,
+                                                               H->fy);
+        *rep = R;
+        rep->converged = 1;
+        return;
+    }
+    R.dt = dt;
+    uint32_t passes = 0, rounds = 0;
+    bool converged = false;
+    while (passes < H->max_passes && rounds < H->max_rounds) {
+        passes++;
+        build_system(H, dt, s);
+        SolveResult S = solve_pass(H, H->precond, H->cfg.solve_tol, (int)(H->max_rounds - rounds), s);
+        rounds += (uint32_t)S.rounds;
+        R.refinements += (uint32_t)S.refinements;
+        R.rel_residual = S.rel;
+        if (!S.ok) break;
+        newton_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->cfg.newton_cell, H->gas, H->C, H->x, H->t, H->u,
+                                                              H->P(S_MOVED), H->P(S_VIOL));
+        H->finalize(S_MOVED, H->grid, s);
+        H->finalize(S_VIOL, H->grid, s);
+        H->read(S_MOVED, 2, s);
+        if (H->hscal[S_MOVED] <= H->cfg.newton_heat * heat0 && H->hscal[S_VIOL] == 0.0) {
+            converged = true;
+            break;
+        }
+    }
+    R.passes = passes;
+    R.rounds = rounds;
+    if (converged) {
+        heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx, H->fy);
+        commit_sums_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->t0, H->u, H->kvac,
+                                                           H->P(S_RAD), H->P(S_GAIN), H->P(S_HELD));
+        H->finalize(S_RAD, H->grid, s);
+        H->finalize(S_GAIN, H->grid, s);
+        H->finalize(S_HELD, H->grid, s);
+        H->read(S_RAD, 3, s);
+        const double rad = H->hscal[S_RAD], gain = H->hscal[S_GAIN], held = H->hscal[S_HELD];
+        const double delta = -(gain + rad) / held;
+        commit_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, delta, H->gas, H->C, H->t, H->t0, U);
+        R.converged = 1;
+        R.delta = delta;
+        R.radiated = rad;
+    } else {
+        limited_scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->C, H->t0,
+                                                             H->lscale);
+        heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, H->lscale, H->fx,
+                                                               H->fy);
+        limited_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->lscale, U,
+                                                             H->P(S_RAD));
+        H->finalize(S_RAD, H->grid, s);
+        H->read(S_RAD, 1, s);
+        R.converged = 0;
+        R.delta = 0.0;
+        R.radiated = H->hscal[S_RAD];
+    }
+    SR_CUDA_TRY(cudaGetLastError());
+    *rep = R;
+}
+
+void heat_first_solve(HeatSolver* H, const float* U, const float* kappa, double dt, uint32_t precond, cudaStream_t s,
+                      double* ms, uint32_t* rounds, double* rel_residual, double* x) {
+    if (precond == SR_PRECOND_LEARNED) throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not loaded"};
+    setup_step(H, U, kappa, s);
+    H->read(S_NGAS, 1, s);
+    H->n_gas = (int)H->hscal[S_NGAS];
+    build_system(H, dt, s);
+    cudaEvent_t a, b;
+    SR_CUDA_TRY(cudaEventCreate(&a));
+    SR_CUDA_TRY(cudaEventCreate(&b));
+    SR_CUDA_TRY(cudaEventRecord(a, s));
+    SolveResult S = solve_pass(H, precond, H->cfg.solve_tol, (int)H->max_rounds, s);
+    SR_CUDA_TRY(cudaEventRecord(b, s));
+    SR_CUDA_TRY(cudaEventSynchronize(b));
+    float t = 0.0f;
+    SR_CUDA_TRY(cudaEventElapsedTime(&t, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (ms) *ms = t;
+    if (rounds) *rounds = (uint32_t)S.rounds;
+    if (rel_residual) *rel_residual = S.rel;
+    if (x) SR_CUDA_TRY(cudaMemcpy(x, H->x, sizeof(double) * H->n, cudaMemcpyDeviceToHost));
+    SR_CUDA_TRY(cudaGetLastError());
+}
