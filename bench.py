@@ -1,0 +1,311 @@
+"""Benchmark of the full per-step field update (hydro + FFT gravity + implicit FLD) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--size S] [--impl ours|reference]
+
+One step = P1 → P2 → P4 (with its half-step gravity solve) → P5 (Newton + FP64-refined MG-PCG to 1e-8) → P8 → P9 on a
+seeded synthetic world of S x S cells (default 2048): a Gaussian disk with lognormal noise in Keplerian rotation, a
+lognormal opacity field with a 32-cell correlation length over six decades, hot spots in the gas (scenes.full_step).
+Under torchrun every rank advances its own world (scene seed = rank): the worlds are independent, no collective on the
+data path, weak scaling. The line also carries the FLD time-to-1e-8 of the 2048² implicit-diffusion configuration
+(scenes.fld) with plain MG-PCG and with Jacobi-PCG.
+
+`--impl reference` times the reference's own CPU algorithm (the f64 twin restated in C, oracle/) on a bounded sample
+of the same workload with every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s hydro+grav+FLD @2048²; FLD time-to-1e-8: learned vs MG-PCG"
+UNIT = "Mcell-steps/s"
+# algorithmic bytes per cell of the fused hydro update kernel with gravity: state in 16 + out 16, P2's g 8,
+# the half-step source 4, φ_mid 4 and g_mid 8
+HYDRO_UPDATE_BYTES_PER_CELL = 56
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.samples.append([v.strip() for v in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for k, name in enumerate(names):
+                if len(s) > 5 + k and s[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel: str, cells: int):
+    """DRAM bytes per launch of `kernel` scaled to `cells`, from the committed ncu summary (profiles/traffic.json)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    k = d.get(kernel)
+    if not k:
+        return None
+    return k["dram_bytes_per_launch"] * cells / k["cells"]
+
+
+def cpu_twin_sample(size: int, steps: int, threads: int):
+    """The oracle's f64 twin on a `size`² world of the benchmark's scene: (Mcell-steps/s, seconds, steps)."""
+    import numpy as np
+
+    import oracle as O
+    from sandbox_reactions_b200 import scenes
+
+    O.set_threads(threads)
+    cfg, P, kappa = scenes.full_step(size)
+    twin = O.Twin(cfg, P.astype(np.float64), kappa.astype(np.float64))
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(steps):
+        twin.step(1)
+        done += 1
+        if time.perf_counter() - t0 > 20.0:
+            break
+    dt = time.perf_counter() - t0
+    return size * size * done / dt / 1e6, dt, done
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    value, secs, done = cpu_twin_sample(args.cpu_size, max(1, args.steps), threads)
+    sample = (f"{done} twin steps of a {args.cpu_size}x{args.cpu_size} world of the benchmark scene "
+              f"(hydro + gravity + FLD, f64, the reference's Jacobi-PCG to 1e-12), {secs:.1f} s on {threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,
+            "warmup": 0, "ms_per_step": 1e3 * secs / max(done, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"full step hydro+gravity+FLD, disk + opacity field + hot spots, "
+                                   f"sample {args.cpu_size}x{args.cpu_size} of the {args.size}x{args.size} case",
+                       "cells": args.cpu_size ** 2, "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def fld_time_to_tol(size: int):
+    """The implicit-diffusion configuration's first system solved to 1e-8 with MG-PCG and Jacobi-PCG (device ms)."""
+    from sandbox_reactions_b200 import scenes
+    from sandbox_reactions_b200.engine import SrError, Step
+
+    cfg, P, kappa = scenes.fld(size)
+    out = {"size": size, "dt": cfg.dt_fixed}
+    with Step(cfg) as s:
+        s.upload(P)
+        s.upload_opacity(kappa)
+        for pc in ("mg", "jacobi", "learned"):
+            try:
+                s.heat_first_solve(cfg.dt_fixed, pc)  # warm-up
+                ms, rounds, rel, _ = s.heat_first_solve(cfg.dt_fixed, pc)
+                out[pc] = {"ms": ms, "rounds": rounds, "rel_residual": rel}
+            except SrError as e:
+                out[pc] = {"unavailable": e.message}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--size", type=int, default=2048)
+    ap.add_argument("--cpu-size", type=int, default=256)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-fld", action="store_true", help="skip the FLD time-to-1e-8 measurement")
+    args = ap.parse_args()
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from sandbox_reactions_b200 import build as lib_build
+
+    if rank == 0:
+        lib_build.build()
+    if dist:
+        dist.barrier()
+    from sandbox_reactions_b200 import scenes
+    from sandbox_reactions_b200.engine import Step, load_library
+
+    load_library()
+    n = args.size
+    cfg, P, kappa = scenes.full_step(n, scene=rank)
+    step = Step(cfg)
+    step.upload(P)
+    step.upload_opacity(kappa)
+    for _ in range(args.warmup):
+        step.run(1)
+
+    # ---- device-resident throughput: K steps timed on the device (events on the library's stream)
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step.set_timing(True)
+    with sampler:
+        step.run(args.steps)
+    torch.cuda.synchronize()
+    cost = step.read_cost()
+    step.set_timing(False)
+    total_ms = cost.total_ms
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * n * n * args.steps / (max_ms / 1e3) / 1e6
+    heat = step.read_heat()
+
+    # ---- end to end through the C ABI: per step the state and κ from pinned host memory in, the state out
+    pin_in = torch.empty((4, n, n), dtype=torch.float32, pin_memory=True)
+    pin_k = torch.empty((n, n), dtype=torch.float32, pin_memory=True)
+    pin_out = torch.empty((4, n, n), dtype=torch.float32, pin_memory=True)
+    pin_in.numpy()[...] = P
+    pin_k.numpy()[...] = kappa
+    e2e_steps = max(1, min(args.steps, 5))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(e2e_steps):
+        step.upload(pin_in.numpy())
+        step.upload_opacity(pin_k.numpy())
+        step.run(1)
+        step.readback(pin_out.numpy())
+    ev1.record()
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * n * n * e2e_steps / (float(t.item()) / 1e3) / 1e6
+
+    fld = None
+    if rank == 0 and not args.no_fld and world == 1:
+        step.close()
+        fld = fld_time_to_tol(2048 if n >= 2048 else n)
+    step.close()
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        upd_ms = cost.hydro_update_ms / max(1, cost.hydro_update_launches)
+        achieved = HYDRO_UPDATE_BYTES_PER_CELL * n * n / (upd_ms / 1e3) / 1e9
+        roofline = {"kernel": "hydro_tile_kernel<kHydroUpdateGrav>", "bound": "hbm", "achieved": achieved,
+                    "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": committed_traffic("hydro_update", n * n), "ms_per_launch": upd_ms,
+                    "algorithmic_bytes_per_cell": HYDRO_UPDATE_BYTES_PER_CELL}
+        cpu = None
+        if world == 1:
+            threads = os.cpu_count() or 1
+            v, secs, done = cpu_twin_sample(args.cpu_size, 50, threads)
+            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{done} f64 twin steps of a {args.cpu_size}x{args.cpu_size} world of the same scene, "
+                             f"{secs:.1f} s"}
+        clocks = sampler.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"full step hydro+gravity+FLD, {n}x{n}, Gaussian disk + lognormal opacity "
+                                   f"(32-cell correlation, 6 decades) + hot spots; FFT {2 * n}x{2 * n}",
+                       "cells": n * n, "parallelism": f"replicas x{world}",
+                       "l2": "working set larger than L2 (state, fields and solver planes > 1 GB)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 5 * 4 * n * n,
+                    "d2h_bytes_per_step": 4 * 4 * n * n, "steps": e2e_steps},
+            "gpu_launches": int(cost.kernel_launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+            "breakdown_ms_per_step": {"gravity": cost.gravity_ms / args.steps, "hydro": cost.hydro_ms / args.steps,
+                                      "heat": cost.heat_ms / args.steps, "floors_dt": cost.dt_ms / args.steps},
+            "heat_last_step": {"passes": heat.passes, "rounds": heat.rounds, "refinements": heat.refinements,
+                               "converged": heat.converged, "rel_residual": heat.rel_residual},
+            "fld_time_to_1e-8": fld,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -134,6 +134,7 @@ typedef struct sr_cost {
     double hydro_update_ms; /* the fused hydro update kernel alone (the roofline kernel) */
     uint32_t hydro_update_launches;
     uint32_t pad2;
+    uint64_t kernel_launches; /* this library's kernel launches during the call */
 } sr_cost;
 
 /* Fills `cfg` with physics.json's shipped constants and the reference's scheme (MC, bounce, γ = 2, self-cell kernel). */

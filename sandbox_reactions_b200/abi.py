@@ -51,7 +51,8 @@ class sr_heat_report(C.Structure):
 class sr_cost(C.Structure):
     _fields_ = [("steps", C.c_uint32), ("pad", C.c_uint32), ("gravity_ms", C.c_double), ("hydro_ms", C.c_double),
                 ("heat_ms", C.c_double), ("floors_ms", C.c_double), ("dt_ms", C.c_double), ("total_ms", C.c_double),
-                ("hydro_update_ms", C.c_double), ("hydro_update_launches", C.c_uint32), ("pad2", C.c_uint32)]
+                ("hydro_update_ms", C.c_double), ("hydro_update_launches", C.c_uint32), ("pad2", C.c_uint32),
+                ("kernel_launches", C.c_uint64)]
 
 
 @dataclass

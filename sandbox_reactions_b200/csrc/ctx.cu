@@ -12,9 +12,15 @@
 #include "heat.cuh"
 #include "hydro.cuh"
 
+#include <atomic>
+
 namespace {
 thread_local std::string g_create_error;
-}
+std::atomic<unsigned long long> g_launches{0};
+}  // namespace
+
+void sr_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+unsigned long long sr_launches() { return g_launches.load(std::memory_order_relaxed); }
 
 struct sr_ctx {
     sr_config cfg{};
@@ -164,6 +170,7 @@ static HydroArgs hydro_args(sr_ctx* c) {
 
 static void run_steps(sr_ctx* c, uint32_t steps) {
     const sr_config& k = c->cfg;
+    const unsigned long long launches0 = sr_launches();
     // event slots per step: 0 start, 1 after P2, 2 hydro update start, 3 hydro update end, 4 after P4, 5 after P5,
     // 6 after P8/P9
     const int E = 7;
@@ -225,6 +232,7 @@ static void run_steps(sr_ctx* c, uint32_t steps) {
             t.total_ms += total;
         }
         t.hydro_update_launches = k.hydro ? steps : 0;
+        t.kernel_launches = sr_launches() - launches0;
     }
 }
 

@@ -247,6 +247,7 @@ void launch_rows(const GravArgs& A, cudaStream_t s) {
     size_t smem = 2 * N * sizeof(float2);
     cudaFuncSetAttribute(grav_rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     grav_rows_kernel<N><<<div_up(A.h, 4), 2 * fft_threads<N>(), smem, s>>>(A);
+    sr_note_launch();
 }
 
 template <int N>
@@ -254,6 +255,7 @@ void launch_columns(const GravArgs& A, cudaStream_t s) {
     size_t smem = N * sizeof(float2);
     cudaFuncSetAttribute(grav_columns_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     grav_columns_kernel<N><<<A.px / 2 + 1, fft_threads<N>(), smem, s>>>(A);
+    sr_note_launch();
 }
 
 template <int N>
@@ -261,6 +263,7 @@ void launch_rows_inverse(const GravArgs& A, cudaStream_t s) {
     size_t smem = 2 * N * sizeof(float2);
     cudaFuncSetAttribute(grav_rows_inverse_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     grav_rows_inverse_kernel<N><<<div_up(A.h + 2, 4), 2 * fft_threads<N>(), smem, s>>>(A);
+    sr_note_launch();
 }
 
 #define SR_FFT_SIZES(X) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096) X(8192)
@@ -458,4 +461,5 @@ void GravPlan::solve(const float* src, float* phi, float* gx, float* gy, cudaStr
     int nb = (int)div_up((unsigned)((n + 3) / 4), 256u);
     nb = nb < 1 ? 1 : (nb > 148 * 8 ? 148 * 8 : nb);
     grav_gradient_kernel<<<nb, 256, 0, s>>>(A);
+    sr_note_launch();
 }

@@ -537,6 +537,7 @@ struct HeatSolver {
 
     void finalize(int slot, int count, cudaStream_t s) {
         finalize_kernel<<<1, RED_THREADS, 0, s>>>(P(slot), count, scal + slot);
+    sr_note_launch();
     }
 
     // Reads device scalars [first, first + count) into hscal (synchronises the stream).
@@ -552,11 +553,14 @@ void setup_step(HeatSolver* H, const float* U, const float* kappa, cudaStream_t 
     const HeatConst& K = H->K;
     heat_cells_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, U, kappa, H->gas, H->t0, H->C, H->kap, H->sig, H->t, H->u,
                                                       H->P(S_HEAT0), H->P(S_NGAS));
+    sr_note_launch();
     H->finalize(S_HEAT0, H->grid, s);
     H->finalize(S_NGAS, H->grid, s);
     const size_t nf = (size_t)(H->w + 1) * H->h + (size_t)H->w * (H->h + 1);
     heat_faces_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(K, H->gas, H->t0, H->kap, H->sig, H->C, H->kx, H->ky);
+    sr_note_launch();
     heat_ksum_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, H->gas, H->kx, H->ky, H->ksum, H->kvac);
+    sr_note_launch();
     H->mg.set_couplings(H->kx, H->ky, H->gas, s);
 }
 
@@ -564,10 +568,12 @@ void setup_step(HeatSolver* H, const float* U, const float* kappa, cudaStream_t 
 void precondition(HeatSolver* H, uint32_t precond, int rz_slot, cudaStream_t s) {
     if (precond == SR_PRECOND_JACOBI) {
         jacobi_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, H->P(rz_slot));
+    sr_note_launch();
         H->finalize(rz_slot, H->grid, s);
     } else {
         H->mg.apply(H->r32, H->z32, s);
         finalize_kernel<<<1, RED_THREADS, 0, s>>>(H->mg.part, H->mg.part_count, H->scal + rz_slot);
+    sr_note_launch();
     }
 }
 
@@ -585,6 +591,7 @@ int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStrea
     H->finalize(S_R32, H->grid, s);  // <r, r> of the scaled residual (partials written by scale_kernel)
     precondition(H, precond, S_RZ0, s);
     pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, -1, S_RZ0, H->z32, H->p32);
+    sr_note_launch();
     H->read(S_R32, 1, s);
     const double rr0 = H->hscal[S_R32];
     if (!(rr0 > 0.0)) return 0;
@@ -593,9 +600,11 @@ int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStrea
     while (it < max_it) {
         const int rz_old = (it & 1) ? S_RZ1 : S_RZ0, rz_new = (it & 1) ? S_RZ0 : S_RZ1;
         spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->P(S_PQ));
+    sr_note_launch();
         H->finalize(S_PQ, H->grid, s);
         pcg_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
                                                           H->P(S_RRI));
+    sr_note_launch();
         H->finalize(S_RRI, H->grid, s);
         it++;
         if (it == next_check || it == max_it) {
@@ -607,6 +616,7 @@ int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStrea
         }
         precondition(H, precond, rz_new, s);
         pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, rz_old, rz_new, H->z32, H->p32);
+    sr_note_launch();
     }
     return it;
 }
@@ -619,6 +629,7 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
     for (int ref = 0; ref < 12; ref++) {
         heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, H->gas, H->diag, H->rhs, H->kx, H->ky, H->x,
                                                                H->r64, H->P(S_RR), H->P(S_BB));
+    sr_note_launch();
         H->finalize(S_RR, H->grid, s);
         H->finalize(S_BB, H->grid, s);
         H->read(S_RR, 2, s);
@@ -633,6 +644,7 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         prev = R.rel;
         const double scale = sqrt(rr / (double)std::max(1, H->n_gas));
         scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->P(S_R32));
+    sr_note_launch();
         const double eta = std::min(0.5, std::max(H->inner_floor, 0.5 * tol / R.rel));
         int it = inner_pcg(H, precond, eta, max_rounds - R.rounds, s);
         if (it < 0) {
@@ -642,6 +654,7 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         R.rounds += it;
         R.refinements++;
         correction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->gas, H->e32, scale, H->x);
+    sr_note_launch();
     }
     return R;
 }
@@ -649,6 +662,7 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
 void build_system(HeatSolver* H, double dt, cudaStream_t s) {
     heat_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->u, H->t0, H->ksum, H->kvac,
                                                        H->diag, H->rhs, H->mg.L[0].c, H->x);
+    sr_note_launch();
     H->mg.coarsen(s);
 }
 
@@ -749,6 +763,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     if (H->cfg.pin_temperature || H->n_gas == 0 || !(dt > 0.0)) {
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx,
                                                                H->fy);
+    sr_note_launch();
         *rep = R;
         rep->converged = 1;
         return;
@@ -766,6 +781,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         if (!S.ok) break;
         newton_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->cfg.newton_cell, H->gas, H->C, H->x, H->t, H->u,
                                                               H->P(S_MOVED), H->P(S_VIOL));
+    sr_note_launch();
         H->finalize(S_MOVED, H->grid, s);
         H->finalize(S_VIOL, H->grid, s);
         H->read(S_MOVED, 2, s);
@@ -778,8 +794,10 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     R.rounds = rounds;
     if (converged) {
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx, H->fy);
+    sr_note_launch();
         commit_sums_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->t0, H->u, H->kvac,
                                                            H->P(S_RAD), H->P(S_GAIN), H->P(S_HELD));
+    sr_note_launch();
         H->finalize(S_RAD, H->grid, s);
         H->finalize(S_GAIN, H->grid, s);
         H->finalize(S_HELD, H->grid, s);
@@ -787,16 +805,20 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         const double rad = H->hscal[S_RAD], gain = H->hscal[S_GAIN], held = H->hscal[S_HELD];
         const double delta = -(gain + rad) / held;
         commit_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, delta, H->gas, H->C, H->t, H->t0, U);
+    sr_note_launch();
         R.converged = 1;
         R.delta = delta;
         R.radiated = rad;
     } else {
         limited_scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->C, H->t0,
                                                              H->lscale);
+    sr_note_launch();
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, H->lscale, H->fx,
                                                                H->fy);
+    sr_note_launch();
         limited_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->lscale, U,
                                                              H->P(S_RAD));
+    sr_note_launch();
         H->finalize(S_RAD, H->grid, s);
         H->read(S_RAD, 1, s);
         R.converged = 0;

@@ -546,21 +546,25 @@ void hydro_launch(int mode, const HydroArgs& A, cudaStream_t s) {
         case kHydroUpdate:
             cudaFuncSetAttribute(hydro_tile_kernel<kHydroUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             hydro_tile_kernel<kHydroUpdate><<<grid, NT, smem, s>>>(A);
+    sr_note_launch();
             break;
         case kHydroSource:
             cudaFuncSetAttribute(hydro_tile_kernel<kHydroSource>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             hydro_tile_kernel<kHydroSource><<<grid, NT, smem, s>>>(A);
+    sr_note_launch();
             break;
         default:
             cudaFuncSetAttribute(hydro_tile_kernel<kHydroUpdateGrav>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
             hydro_tile_kernel<kHydroUpdateGrav><<<grid, NT, smem, s>>>(A);
+    sr_note_launch();
             break;
     }
 }
 
 void hydro_finalize_launch(const HydroArgs& A, int take_back, cudaStream_t s) {
     hydro_finalize_kernel<<<1, 256, 0, s>>>(A, hydro_blocks(A.H.w, A.H.h), take_back);
+    sr_note_launch();
 }
 
 // ------------------------------------------------------------------------------------------------ P8 + P9
@@ -673,7 +677,10 @@ void floors_dt_launch(const HydroConst& H, float* U, const float* gx, const floa
                       DtRecord* rec, cudaStream_t s) {
     int nb = floors_dt_blocks(H.w, H.h);
     floors_dt_kernel<<<nb, 256, 0, s>>>(H, U, gx, gy, do_floors, part_rate, part_g, part_nf);
+    sr_note_launch();
     dt_finalize_kernel<<<1, 32, 0, s>>>(nb, part_rate, part_g, part_nf, cfl, eta_g, dt_fixed, dt_cap, rec);
+    sr_note_launch();
 }
 
-void dt_advance_launch(DtRecord* rec, cudaStream_t s) { dt_advance_kernel<<<1, 32, 0, s>>>(rec); }
+void dt_advance_launch(DtRecord* rec, cudaStream_t s) { dt_advance_kernel<<<1, 32, 0, s>>>(rec);
+    sr_note_launch(); }

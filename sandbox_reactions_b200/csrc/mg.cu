@@ -343,6 +343,7 @@ void launch_smooth(const MgLevel& L, const float* xc, int wc, float omega, doubl
     cudaFuncSetAttribute(mg_smooth_kernel<NS, PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid(div_up(L.w, SX), div_up(L.h, SY));
     mg_smooth_kernel<NS, PRE><<<grid, SMOOTH_THREADS, smem, s>>>(L, xc, wc, omega, part);
+    sr_note_launch();
 }
 
 void smooth(int nu, bool pre, const MgLevel& L, const float* xc, int wc, float omega, double* part, cudaStream_t s) {
@@ -424,11 +425,13 @@ size_t Multigrid::bytes() const {
 
 void Multigrid::set_couplings(const double* kx, const double* ky, const uint8_t* gas, cudaStream_t s) {
     mg_couplings0_kernel<<<grid_for((size_t)L[0].w * L[0].h), 256, 0, s>>>(L[0], kx, ky, gas);
+    sr_note_launch();
 }
 
 void Multigrid::coarsen(cudaStream_t s) {
     for (int l = 1; l < nlevels; l++)
         mg_coarsen_kernel<<<grid_for((size_t)L[l].w * L[l].h), 256, 0, s>>>(L[l - 1], L[l]);
+    sr_note_launch();
 }
 
 void Multigrid::apply(const float* r, float* z, cudaStream_t s) {
@@ -437,6 +440,7 @@ void Multigrid::apply(const float* r, float* z, cudaStream_t s) {
     for (int l = 0; l < tail; l++) {
         smooth(pre, true, L[l], nullptr, 0, omega, nullptr, s);
         mg_restrict_kernel<<<grid_for((size_t)L[l + 1].w * L[l + 1].h), 256, 0, s>>>(L[l], L[l + 1]);
+    sr_note_launch();
     }
     TailArgs T;
     T.t = tail;
@@ -447,6 +451,7 @@ void Multigrid::apply(const float* r, float* z, cudaStream_t s) {
     for (int l = 0; l < nlevels; l++) T.L[l] = L[l];
     T.part = tail == 0 ? part : nullptr;
     mg_tail_kernel<<<1, TAIL_THREADS, tail_smem(*this), s>>>(T);
+    sr_note_launch();
     for (int l = tail - 1; l >= 0; l--)
         smooth(post, false, L[l], L[l + 1].x2, L[l + 1].w, omega, l == 0 ? part : nullptr, s);
 }
