@@ -93,7 +93,9 @@ typedef struct sr_config {
     double newton_cell;       /* ... and every |ΔT| <= newton_cell T */
     double dt_fixed;          /* > 0: every step runs on this Δt instead of the CFL/gravity one */
     double dt_cap;            /* > 0: Δt_{n+1} = min(Δt_{n+1}, dt_cap) (reference/mod.rs:213-216) */
-    double reserved_d[4];
+    double mg_omega;          /* weight of the multigrid's coarse correction (0: the library's default) */
+    double inner_tol;         /* smallest residual reduction asked of one FP32 inner solve (0: default 1e-5) */
+    double reserved_d[2];
 } sr_config;
 
 /* Δt record (crates/sr-engine/src/step/dt.rs:51-61). */

@@ -33,7 +33,7 @@ class sr_config(C.Structure):
         ("softening", C.c_double), ("a_r", C.c_double), ("c_sb", C.c_double), ("kappa0", C.c_double),
         ("k_cond", C.c_double), ("chi", C.c_double), ("solve_tol", C.c_double), ("newton_heat", C.c_double),
         ("newton_cell", C.c_double), ("dt_fixed", C.c_double), ("dt_cap", C.c_double),
-        ("reserved_d", C.c_double * 4),
+        ("mg_omega", C.c_double), ("inner_tol", C.c_double), ("reserved_d", C.c_double * 2),
     ]
 
 
@@ -91,9 +91,11 @@ class Config:
     chi: float = 0.0
     solve_tol: float = 1e-8
     newton_heat: float = 1e-9
-    newton_cell: float = 1e-7
+    newton_cell: float = 1e-6
     dt_fixed: float = 0.0
     dt_cap: float = 0.0
+    mg_omega: float = 0.0
+    inner_tol: float = 0.0
 
     def to_c(self) -> sr_config:
         c = sr_config()

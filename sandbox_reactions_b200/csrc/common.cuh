@@ -112,5 +112,6 @@ SR_HOST_DEVICE void euler_flux(const Prim& p, float energy, int dir, float* f) {
 // ------------------------------------------------------------------------------------------------ launch helpers
 // Every kernel launch of the library is counted (sr_cost.kernel_launches reports the count of an sr_step call).
 void sr_note_launch();
+void sr_note_launches(long long n);
 unsigned long long sr_launches();
 static inline unsigned div_up(unsigned a, unsigned b) { return (a + b - 1) / b; }

@@ -20,6 +20,7 @@ std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
 void sr_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void sr_note_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 unsigned long long sr_launches() { return g_launches.load(std::memory_order_relaxed); }
 
 struct sr_ctx {
@@ -271,7 +272,7 @@ void sr_config_default(sr_config* c) {
     c->chi = 0.0;
     c->solve_tol = 1e-8;
     c->newton_heat = 1e-9;
-    c->newton_cell = 1e-7;
+    c->newton_cell = 1e-6;
 }
 
 uint32_t sr_abi_version(void) { return SR_ABI_VERSION; }

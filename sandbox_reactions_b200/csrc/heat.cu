@@ -14,12 +14,22 @@
 
 #include "heat.cuh"
 #include "mg.cuh"
+#include "reduce.cuh"
 
 namespace {
 
 constexpr int RED_THREADS = 256;
-constexpr int MAX_PART = 4096;
-enum Slot { S_NGAS, S_DT, S_HEAT0, S_RR, S_BB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1, S_MOVED, S_VIOL, S_RAD, S_GAIN, S_HELD, S_COUNT };
+constexpr int MAX_PART = 4096;    // most CTAs of a grid-stride heat kernel
+constexpr int PART_CAP = 16384;   // partials per reduced value (the level-0 smoother's CTAs included)
+enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1,
+            S_MOVED, S_VIOL, S_RAD, S_GAIN, S_HELD, S_COUNT };
+
+// Where a kernel's grid sum goes: the partials buffer, the ticket counter and the device scalar(s).
+struct Red {
+    double* part;
+    unsigned* counter;
+    double* out;
+};
 
 struct HeatConst {
     int w, h;
@@ -37,40 +47,10 @@ __device__ __forceinline__ double dt_du(const HeatConst& K, double t) {
     return K.chi > 0.0 ? 1.0 : 1.0 / (4.0 * K.a_r * ((t * t) * t));
 }
 
-// Block reduction of a double into part[blockIdx.x] (fixed order).
-__device__ __forceinline__ void block_sum(double v, double* part) {
-    __shared__ double red[32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += red[q];
-        part[blockIdx.x] = t;
-    }
-    __syncthreads();
-}
-
-__global__ void finalize_kernel(const double* __restrict__ part, int count, double* out) {
-    __shared__ double sd[RED_THREADS];
-    const int tid = threadIdx.x;
-    const int per = (count + RED_THREADS - 1) / RED_THREADS;
-    double acc = 0.0;
-    for (int b = tid * per; b < min(count, (tid + 1) * per); b++) acc += part[b];
-    sd[tid] = acc;
-    __syncthreads();
-    if (tid == 0) {
-        double t = 0.0;
-        for (int k = 0; k < RED_THREADS; k++) t += sd[k];
-        *out = t;
-    }
-}
-
 // ---- step set-up: the sides (heat.rs:215-226), the faces' D_f (heat.rs:263-294), Σ_f k and its vacuum part
 __global__ void heat_cells_kernel(HeatConst K, const float* __restrict__ U, const float* __restrict__ kappa,
                                   uint8_t* gas, double* t0, double* C, float* kap, float* sig, double* t, double* u,
-                                  double* part, double* part_gas) {
+                                  Red R) {
     const size_t n = (size_t)K.w * K.h;
     double acc = 0.0, ngas = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -101,8 +81,8 @@ __global__ void heat_cells_kernel(HeatConst K, const float* __restrict__ U, cons
         acc += C[i] * T;
         ngas += 1.0;
     }
-    block_sum(acc, part);
-    block_sum(ngas, part_gas);
+    const double v[2] = {acc, ngas};
+    grid_sum_last<2>(v, R.part, R.counter, R.out);
 }
 
 struct Side {
@@ -218,17 +198,20 @@ __global__ void heat_ksum_kernel(HeatConst K, const uint8_t* __restrict__ gas, c
     }
 }
 
-// ---- a Newton pass's system at the iterate (heat.rs:476-489) and level 0's excess c = c_i + Σ_vac D_f (FP32)
+// ---- a Newton pass's system at the iterate (heat.rs:476-489), kept as its mass term c = c_i + Σ_vac D_f (the
+// diagonal less the couplings to gas neighbours, f64; FP32 copy as level 0's c) so that A x = c x + Σ D (x_i - x_j)
+// is evaluated without cancellation; partials of the two measures' bounds, Σ c_i u² and Σ (C/Δt) T² (heat.rs:480-487).
 __global__ void heat_system_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
                                    const double* __restrict__ C, const double* __restrict__ t,
                                    const double* __restrict__ u, const double* __restrict__ t0,
-                                   const double* __restrict__ ksum, const double* __restrict__ kvac, double* diag,
-                                   double* rhs, float* c0, double* x) {
+                                   const double* __restrict__ kvac, double* c64, double* rhs, float* c0, double* x,
+                                   Red R) {
     const size_t n = (size_t)K.w * K.h;
     const double u_vac = u_of(K, K.t_floor);
+    double ub = 0.0, tb = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) {
-            diag[i] = 1.0;
+            c64[i] = 1.0;
             rhs[i] = 0.0;
             c0[i] = 1.0f;
             x[i] = 0.0;
@@ -236,43 +219,69 @@ __global__ void heat_system_kernel(HeatConst K, double dt, const uint8_t* __rest
         }
         const double heat = C[i] / dt;
         const double ci = heat * dt_du(K, t[i]);
-        diag[i] = ci + ksum[i];
+        c64[i] = ci + kvac[i];
         rhs[i] = ci * u[i] - heat * (t[i] - t0[i]) + kvac[i] * u_vac;
         c0[i] = (float)(ci + kvac[i]);
         x[i] = u[i];
+        ub += ci * u[i] * u[i];
+        tb += heat * t[i] * t[i];
     }
+    const double v[2] = {ub, tb};
+    grid_sum_last<2>(v, R.part, R.counter, R.out);
 }
 
-// r = b - A x in FP64 with partials of <r, r> and <b, b>.
-__global__ void heat_residual64_kernel(HeatConst K, const uint8_t* __restrict__ gas, const double* __restrict__ diag,
-                                       const double* __restrict__ rhs, const double* __restrict__ kx,
-                                       const double* __restrict__ ky, const double* __restrict__ x, double* r,
-                                       double* part_rr, double* part_bb) {
+// r = b - A x in FP64, A x = c x + Σ_gas D (x_i - x_j), with partials of <r, r>, <b, b> and the reference's two
+// measures (heat.rs:413-447): rᵀD⁻¹r and the heat measure Σ (C/Δt)(r (dT/du) / D_ii)².
+__global__ void heat_residual64_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+                                       const double* __restrict__ c64, const double* __restrict__ rhs,
+                                       const double* __restrict__ kx, const double* __restrict__ ky,
+                                       const double* __restrict__ C, const double* __restrict__ t,
+                                       const double* __restrict__ x, double* r, Red R) {
     const int w = K.w, h = K.h;
     const size_t n = (size_t)w * h;
-    double rr = 0.0, bb = 0.0;
+    double rr = 0.0, bb = 0.0, gg = 0.0, hh = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) {
             r[i] = 0.0;
             continue;
         }
         const int xx = (int)(i % w), y = (int)(i / w);
-        double s = diag[i] * x[i];
-        if (xx > 0 && gas[i - 1]) s -= kx[(size_t)y * (w + 1) + xx] * x[i - 1];
-        if (xx + 1 < w && gas[i + 1]) s -= kx[(size_t)y * (w + 1) + xx + 1] * x[i + 1];
-        if (y > 0 && gas[i - w]) s -= ky[(size_t)y * w + xx] * x[i - w];
-        if (y + 1 < h && gas[i + w]) s -= ky[(size_t)(y + 1) * w + xx] * x[i + w];
+        const double xi = x[i];
+        double s = c64[i] * xi, d = c64[i];
+        if (xx > 0 && gas[i - 1]) {
+            const double k = kx[(size_t)y * (w + 1) + xx];
+            s += k * (xi - x[i - 1]);
+            d += k;
+        }
+        if (xx + 1 < w && gas[i + 1]) {
+            const double k = kx[(size_t)y * (w + 1) + xx + 1];
+            s += k * (xi - x[i + 1]);
+            d += k;
+        }
+        if (y > 0 && gas[i - w]) {
+            const double k = ky[(size_t)y * w + xx];
+            s += k * (xi - x[i - w]);
+            d += k;
+        }
+        if (y + 1 < h && gas[i + w]) {
+            const double k = ky[(size_t)(y + 1) * w + xx];
+            s += k * (xi - x[i + w]);
+            d += k;
+        }
         const double ri = rhs[i] - s;
         r[i] = ri;
         rr += ri * ri;
         bb += rhs[i] * rhs[i];
+        gg += ri * ri / d;
+        const double e = ri * dt_du(K, t[i]) / d;
+        hh += C[i] / dt * e * e;
     }
-    block_sum(rr, part_rr);
-    block_sum(bb, part_bb);
+    const double v[4] = {rr, bb, gg, hh};
+    grid_sum_last<4>(v, R.part, R.counter, R.out);
 }
 
 __global__ void scale_kernel(size_t n, const double* __restrict__ r64, double inv_scale, float* r32, float* e32,
-                             double* part) {
+                             Red R) {
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float v = (float)(r64[i] * inv_scale);
@@ -280,11 +289,11 @@ __global__ void scale_kernel(size_t n, const double* __restrict__ r64, double in
         e32[i] = 0.0f;
         acc += (double)v * v;
     }
-    block_sum(acc, part);
+    grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
-// q = A p on level 0's FP32 operator (diagonal c + Σ couplings), partials of <p, q>.
-__global__ void spmv_kernel(MgLevel L, const float* __restrict__ p, float* q, double* part) {
+// q = A p on level 0's FP32 operator in difference form, c p_i + Σ d (p_i - p_j); partials of <p, q>.
+__global__ void spmv_kernel(MgLevel L, const float* __restrict__ p, float* q, Red R) {
     const int w = L.w, h = L.h;
     const size_t n = (size_t)w * h;
     double acc = 0.0;
@@ -292,23 +301,22 @@ __global__ void spmv_kernel(MgLevel L, const float* __restrict__ p, float* q, do
         const int x = (int)(i % w), y = (int)(i / w);
         float v = 0.0f;
         if (L.mask[i]) {
-            const float dl = x > 0 ? L.dx[i - 1] : 0.0f, du = y > 0 ? L.dy[i - w] : 0.0f;
-            const float dr = L.dx[i], dd = L.dy[i];
-            v = (L.c[i] + dl + dr + du + dd) * p[i];
-            if (x > 0) v -= dl * p[i - 1];
-            if (x + 1 < w) v -= dr * p[i + 1];
-            if (y > 0) v -= du * p[i - w];
-            if (y + 1 < h) v -= dd * p[i + w];
+            const float pi = p[i];
+            v = L.c[i] * pi;
+            if (x > 0) v += L.dx[i - 1] * (pi - p[i - 1]);
+            if (x + 1 < w) v += L.dx[i] * (pi - p[i + 1]);
+            if (y > 0) v += L.dy[i - w] * (pi - p[i - w]);
+            if (y + 1 < h) v += L.dy[i] * (pi - p[i + w]);
         }
         q[i] = v;
         acc += (double)p[i] * v;
     }
-    block_sum(acc, part);
+    grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
 // e += α p, r -= α q (α = <r,z>/<p,q> from the device scalars), partials of <r, r>.
 __global__ void pcg_update_kernel(size_t n, const double* __restrict__ scal, int rz_slot, const float* __restrict__ p,
-                                  const float* __restrict__ q, float* e, float* r, double* part) {
+                                  const float* __restrict__ q, float* e, float* r, Red R) {
     const float alpha = (float)(scal[rz_slot] / scal[S_PQ]);
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -317,7 +325,7 @@ __global__ void pcg_update_kernel(size_t n, const double* __restrict__ scal, int
         r[i] = ri;
         acc += (double)ri * ri;
     }
-    block_sum(acc, part);
+    grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
 // p = z + β p (β = <r,z>_new / <r,z>_old); the first direction (old slot < 0) is p = z.
@@ -329,7 +337,7 @@ __global__ void pcg_direction_kernel(size_t n, const double* __restrict__ scal, 
 }
 
 // z = r / diag (Jacobi), partials of <r, z>.
-__global__ void jacobi_kernel(MgLevel L, const float* __restrict__ r, float* z, double* part) {
+__global__ void jacobi_kernel(MgLevel L, const float* __restrict__ r, float* z, Red R) {
     const int w = L.w, h = L.h;
     const size_t n = (size_t)w * h;
     double acc = 0.0;
@@ -340,7 +348,7 @@ __global__ void jacobi_kernel(MgLevel L, const float* __restrict__ r, float* z, 
         z[i] = zi;
         acc += (double)r[i] * zi;
     }
-    block_sum(acc, part);
+    grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
 __global__ void correction_kernel(size_t n, const uint8_t* __restrict__ gas, const float* __restrict__ e,
@@ -353,7 +361,7 @@ __global__ void correction_kernel(size_t n, const uint8_t* __restrict__ gas, con
 // by more than newton_cell of their T.
 __global__ void newton_update_kernel(HeatConst K, double cell_tol, const uint8_t* __restrict__ gas,
                                      const double* __restrict__ C, const double* __restrict__ x, double* t, double* u,
-                                     double* part_moved, double* part_viol) {
+                                     Red R) {
     const size_t n = (size_t)K.w * K.h;
     const double u_vac = u_of(K, K.t_floor);
     double moved = 0.0, viol = 0.0;
@@ -368,8 +376,8 @@ __global__ void newton_update_kernel(HeatConst K, double cell_tol, const uint8_t
         t[i] = nx;
         u[i] = u_of(K, nx);
     }
-    block_sum(moved, part_moved);
-    block_sum(viol, part_viol);
+    const double v[2] = {moved, viol};
+    grid_sum_last<2>(v, R.part, R.counter, R.out);
 }
 
 // F = -k (v_b - v_a) at every face (heat.rs:338-361), v = u on gas cells, u_vac elsewhere; FP32 out.
@@ -416,7 +424,7 @@ __global__ void heat_flux_kernel(HeatConst K, const uint8_t* __restrict__ gas, c
 __global__ void commit_sums_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
                                    const double* __restrict__ C, const double* __restrict__ t,
                                    const double* __restrict__ t0, const double* __restrict__ u,
-                                   const double* __restrict__ kvac, double* p_rad, double* p_gain, double* p_held) {
+                                   const double* __restrict__ kvac, Red R) {
     const size_t n = (size_t)K.w * K.h;
     const double u_vac = u_of(K, K.t_floor);
     double rad = 0.0, gain = 0.0, held = 0.0;
@@ -426,9 +434,8 @@ __global__ void commit_sums_kernel(HeatConst K, double dt, const uint8_t* __rest
         gain += C[i] * (t[i] - t0[i]);
         held += C[i] * t[i];
     }
-    block_sum(rad, p_rad);
-    block_sum(gain, p_gain);
-    block_sum(held, p_held);
+    const double v[3] = {rad, gain, held};
+    grid_sum_last<3>(v, R.part, R.counter, R.out);
 }
 
 // E_i += C_i ((1 + δ) T_i - T_i⁰) (heat.rs:532-535).
@@ -472,7 +479,7 @@ __global__ void limited_scale_kernel(HeatConst K, double dt, const uint8_t* __re
 __global__ void limited_apply_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
                                      const double* __restrict__ kx, const double* __restrict__ ky,
                                      const double* __restrict__ u, const double* __restrict__ scale, float* U,
-                                     double* p_rad) {
+                                     Red R) {
     const int w = K.w, h = K.h;
     const size_t n = (size_t)w * h;
     const double u_vac = u_of(K, K.t_floor);
@@ -501,7 +508,7 @@ __global__ void limited_apply_kernel(HeatConst K, double dt, const uint8_t* __re
             if (!(nb[f] >= 0 && gas[nb[f]])) rad += dt * out[f];
         U[3 * n + i] = (float)((double)U[3 * n + i] - dt * (((out[0] + out[1]) + out[2]) + out[3]));
     }
-    block_sum(rad, p_rad);
+    grid_sum_last1(rad, R.part, R.counter, R.out);
 }
 
 int grid_for(size_t n) {
@@ -510,6 +517,11 @@ int grid_for(size_t n) {
 }
 
 }  // namespace
+
+struct RoundGraph {
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;  // kernel nodes in the graph
+};
 
 struct HeatSolver {
     sr_config cfg{};
@@ -520,25 +532,23 @@ struct HeatSolver {
     uint32_t precond = SR_PRECOND_MG;
     uint32_t max_passes = 128, max_rounds = 4096;
     double inner_floor = 1e-5;  // the smallest residual reduction asked of one inner FP32 solve
+    bool use_graphs = true;
     uint8_t* gas = nullptr;
     double *t0 = nullptr, *C = nullptr, *t = nullptr, *u = nullptr, *kx = nullptr, *ky = nullptr;
-    double *ksum = nullptr, *kvac = nullptr, *diag = nullptr, *rhs = nullptr, *x = nullptr, *r64 = nullptr;
+    double *ksum = nullptr, *kvac = nullptr, *c64 = nullptr, *rhs = nullptr, *x = nullptr, *r64 = nullptr;
     double* lscale = nullptr;
     float *kap = nullptr, *sig = nullptr;
     float *r32 = nullptr, *e32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr;
     float *fx = nullptr, *fy = nullptr;
-    double* part = nullptr;  // S_COUNT slots of MAX_PART partials
-    double* scal = nullptr;  // S_COUNT device scalars
-    double* hscal = nullptr; // pinned host copy
+    double* part = nullptr;      // grid-sum partials: 4 x PART_CAP
+    unsigned* counter = nullptr;  // grid-sum ticket
+    double* scal = nullptr;       // S_COUNT device scalars
+    double* hscal = nullptr;      // pinned host copy
     Multigrid mg;
     int n_gas = 0;
+    RoundGraph graphs[3][2];      // one PCG round per preconditioner and <r,z> slot parity
 
-    double* P(int slot) { return part + (size_t)slot * MAX_PART; }
-
-    void finalize(int slot, int count, cudaStream_t s) {
-        finalize_kernel<<<1, RED_THREADS, 0, s>>>(P(slot), count, scal + slot);
-    sr_note_launch();
-    }
+    Red red(int slot) { return Red{part, counter, scal + slot}; }
 
     // Reads device scalars [first, first + count) into hscal (synchronises the stream).
     void read(int first, int count, cudaStream_t s) {
@@ -552,10 +562,8 @@ namespace {
 void setup_step(HeatSolver* H, const float* U, const float* kappa, cudaStream_t s) {
     const HeatConst& K = H->K;
     heat_cells_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, U, kappa, H->gas, H->t0, H->C, H->kap, H->sig, H->t, H->u,
-                                                      H->P(S_HEAT0), H->P(S_NGAS));
+                                                      H->red(S_HEAT0));
     sr_note_launch();
-    H->finalize(S_HEAT0, H->grid, s);
-    H->finalize(S_NGAS, H->grid, s);
     const size_t nf = (size_t)(H->w + 1) * H->h + (size_t)H->w * (H->h + 1);
     heat_faces_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(K, H->gas, H->t0, H->kap, H->sig, H->C, H->kx, H->ky);
     sr_note_launch();
@@ -564,17 +572,50 @@ void setup_step(HeatSolver* H, const float* U, const float* kappa, cudaStream_t 
     H->mg.set_couplings(H->kx, H->ky, H->gas, s);
 }
 
-// z = M r with partials of <r, z> into slot `rz_slot`.
+// z = M r, and <r, z> into scalar `rz_slot`.
 void precondition(HeatSolver* H, uint32_t precond, int rz_slot, cudaStream_t s) {
     if (precond == SR_PRECOND_JACOBI) {
-        jacobi_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, H->P(rz_slot));
-    sr_note_launch();
-        H->finalize(rz_slot, H->grid, s);
+        jacobi_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, H->red(rz_slot));
+        sr_note_launch();
     } else {
-        H->mg.apply(H->r32, H->z32, s);
-        finalize_kernel<<<1, RED_THREADS, 0, s>>>(H->mg.part, H->mg.part_count, H->scal + rz_slot);
-    sr_note_launch();
+        H->mg.apply(H->r32, H->z32, H->part, H->counter, H->scal + rz_slot, s);
     }
+}
+
+// One PCG round: q = A p, α, e += α p, r -= α q, z = M r, β, p = z + β p. `parity` picks the <r,z> slots.
+void round_launches(HeatSolver* H, uint32_t precond, int parity, cudaStream_t s) {
+    const int rz_old = parity ? S_RZ1 : S_RZ0, rz_new = parity ? S_RZ0 : S_RZ1;
+    spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->red(S_PQ));
+    sr_note_launch();
+    pcg_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
+                                                      H->red(S_RRI));
+    sr_note_launch();
+    precondition(H, precond, rz_new, s);
+    pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, rz_new, H->z32, H->p32);
+    sr_note_launch();
+}
+
+// A round as one CUDA graph launch (captured once per preconditioner and parity; every pointer it reads is fixed).
+void run_round(HeatSolver* H, uint32_t precond, int parity, cudaStream_t s) {
+    if (!H->use_graphs) {
+        round_launches(H, precond, parity, s);
+        return;
+    }
+    RoundGraph& g = H->graphs[precond][parity];
+    if (!g.exec) {
+        const long long before = (long long)sr_launches();
+        cudaGraph_t graph;
+        SR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        round_launches(H, precond, parity, s);
+        SR_CUDA_TRY(cudaStreamEndCapture(s, &graph));
+        cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        SR_CUDA_TRY(e);
+        g.launches = (long long)sr_launches() - before;
+        sr_note_launches(-g.launches);  // captured, not launched
+    }
+    SR_CUDA_TRY(cudaGraphLaunch(g.exec, s));
+    sr_note_launches(g.launches);
 }
 
 struct SolveResult {
@@ -587,25 +628,16 @@ struct SolveResult {
 // PCG on A32 e = r32 from e = 0 to a residual reduction `eta` or `max_it` rounds. Returns the rounds, or -1 on a
 // breakdown (a non-positive or non-finite curvature).
 int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStream_t s) {
-    const size_t n = H->n;
-    H->finalize(S_R32, H->grid, s);  // <r, r> of the scaled residual (partials written by scale_kernel)
     precondition(H, precond, S_RZ0, s);
-    pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, -1, S_RZ0, H->z32, H->p32);
+    pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, -1, S_RZ0, H->z32, H->p32);
     sr_note_launch();
-    H->read(S_R32, 1, s);
+    H->read(S_R32, 1, s);  // <r, r> of the scaled residual (written by scale_kernel)
     const double rr0 = H->hscal[S_R32];
     if (!(rr0 > 0.0)) return 0;
     int it = 0;
     int next_check = 1;
     while (it < max_it) {
-        const int rz_old = (it & 1) ? S_RZ1 : S_RZ0, rz_new = (it & 1) ? S_RZ0 : S_RZ1;
-        spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->P(S_PQ));
-    sr_note_launch();
-        H->finalize(S_PQ, H->grid, s);
-        pcg_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
-                                                          H->P(S_RRI));
-    sr_note_launch();
-        H->finalize(S_RRI, H->grid, s);
+        run_round(H, precond, it & 1, s);
         it++;
         if (it == next_check || it == max_it) {
             H->read(S_PQ, 2, s);  // S_PQ, S_RRI
@@ -614,38 +646,40 @@ int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStrea
             if (rr <= eta * eta * rr0) break;
             next_check = it < 4 ? it + 1 : it + 4;
         }
-        precondition(H, precond, rz_new, s);
-        pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(n, H->scal, rz_old, rz_new, H->z32, H->p32);
-    sr_note_launch();
     }
     return it;
 }
 
-// The pass's system to ||b - A x|| <= tol ||b|| by FP64 refinement around FP32 PCG; x starts at the iterate.
-SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_rounds, cudaStream_t s) {
+// The pass's system by FP64 refinement around FP32 PCG, x starting at the iterate, until the plain relative residual
+// ||b - A x|| / ||b|| and the reference's two measures (rᵀD⁻¹r against Σ c_i u², the heat measure against
+// Σ (C/Δt) T², heat.rs:480-487 and 422-431) are all within `tol`; stops early when a refinement no longer halves the
+// worst of the three ratios, or past `max_rounds`.
+SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_rounds, double dt, cudaStream_t s) {
     SolveResult R;
     const HeatConst& K = H->K;
     double prev = INFINITY;
-    for (int ref = 0; ref < 12; ref++) {
-        heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, H->gas, H->diag, H->rhs, H->kx, H->ky, H->x,
-                                                               H->r64, H->P(S_RR), H->P(S_BB));
-    sr_note_launch();
-        H->finalize(S_RR, H->grid, s);
-        H->finalize(S_BB, H->grid, s);
-        H->read(S_RR, 2, s);
-        const double rr = H->hscal[S_RR], bb = H->hscal[S_BB];
-        if (!isfinite(rr) || !isfinite(bb)) {
+    const double ub = H->hscal[S_UB], tb = H->hscal[S_TB];
+    for (int ref = 0; ref < 16; ref++) {
+        heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, dt, H->gas, H->c64, H->rhs, H->kx, H->ky, H->C,
+                                                               H->t, H->x, H->r64, H->red(S_RR));
+        sr_note_launch();
+        H->read(S_RR, 4, s);
+        const double rr = H->hscal[S_RR], bb = H->hscal[S_BB], gam = H->hscal[S_GAM], hm = H->hscal[S_HM];
+        if (!isfinite(rr) || !isfinite(bb) || !isfinite(gam) || !isfinite(hm)) {
             R.ok = false;
             return R;
         }
         R.rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
-        if (R.rel <= tol || rr == 0.0) return R;
-        if (R.rel > 0.5 * prev || R.rounds >= max_rounds) return R;  // stagnating, or out of rounds
-        prev = R.rel;
+        double worst = R.rel / tol;
+        if (ub > 0.0) worst = std::max(worst, sqrt(gam / ub) / tol);
+        if (tb > 0.0) worst = std::max(worst, sqrt(hm / tb) / tol);
+        if (worst <= 1.0 || rr == 0.0) return R;
+        if (worst > 0.5 * prev || R.rounds >= max_rounds) return R;  // stagnating, or out of rounds
+        prev = worst;
         const double scale = sqrt(rr / (double)std::max(1, H->n_gas));
-        scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->P(S_R32));
-    sr_note_launch();
-        const double eta = std::min(0.5, std::max(H->inner_floor, 0.5 * tol / R.rel));
+        scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->red(S_R32));
+        sr_note_launch();
+        const double eta = std::min(0.5, std::max(H->inner_floor, 0.5 / worst));
         int it = inner_pcg(H, precond, eta, max_rounds - R.rounds, s);
         if (it < 0) {
             R.ok = false;
@@ -654,16 +688,18 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         R.rounds += it;
         R.refinements++;
         correction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->gas, H->e32, scale, H->x);
-    sr_note_launch();
+        sr_note_launch();
     }
     return R;
 }
 
+// A pass's system and its measures' bounds (read to the host), then every coarse level and the coarsest inverse.
 void build_system(HeatSolver* H, double dt, cudaStream_t s) {
-    heat_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->u, H->t0, H->ksum, H->kvac,
-                                                       H->diag, H->rhs, H->mg.L[0].c, H->x);
+    heat_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->u, H->t0, H->kvac, H->c64,
+                                                       H->rhs, H->mg.L[0].c, H->x, H->red(S_UB));
     sr_note_launch();
     H->mg.coarsen(s);
+    H->read(S_UB, 2, s);
 }
 
 }  // namespace
@@ -675,6 +711,7 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         H->w = (int)cfg.width;
         H->h = (int)cfg.height;
         H->n = (size_t)H->w * H->h;
+        SR_REQUIRE(cfg.precond != SR_PRECOND_LEARNED, "the learned preconditioner is loaded after creation");
         H->precond = cfg.precond;
         H->max_passes = cfg.max_passes ? cfg.max_passes : 128;
         H->max_rounds = cfg.max_rounds ? cfg.max_rounds : 4096;
@@ -695,7 +732,7 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         H->grid = grid_for(H->n);
         const size_t n = H->n, nx = (size_t)(H->w + 1) * H->h, ny = (size_t)H->w * (H->h + 1);
         SR_CUDA_TRY(cudaMalloc(&H->gas, n));
-        double** d64[] = {&H->t0, &H->C, &H->t, &H->u, &H->ksum, &H->kvac, &H->diag, &H->rhs, &H->x, &H->r64,
+        double** d64[] = {&H->t0, &H->C, &H->t, &H->u, &H->ksum, &H->kvac, &H->c64, &H->rhs, &H->x, &H->r64,
                           &H->lscale};
         for (double** p : d64) SR_CUDA_TRY(cudaMalloc(p, sizeof(double) * n));
         SR_CUDA_TRY(cudaMalloc(&H->kx, sizeof(double) * nx));
@@ -706,11 +743,16 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         SR_CUDA_TRY(cudaMalloc(&H->fy, sizeof(float) * ny));
         SR_CUDA_TRY(cudaMemset(H->fx, 0, sizeof(float) * nx));
         SR_CUDA_TRY(cudaMemset(H->fy, 0, sizeof(float) * ny));
-        SR_CUDA_TRY(cudaMalloc(&H->part, sizeof(double) * MAX_PART * S_COUNT));
+        SR_CUDA_TRY(cudaMalloc(&H->part, sizeof(double) * 4 * PART_CAP));
+        SR_CUDA_TRY(cudaMalloc(&H->counter, sizeof(unsigned)));
+        SR_CUDA_TRY(cudaMemset(H->counter, 0, sizeof(unsigned)));
         SR_CUDA_TRY(cudaMalloc(&H->scal, sizeof(double) * S_COUNT));
         SR_CUDA_TRY(cudaMemset(H->scal, 0, sizeof(double) * S_COUNT));
         SR_CUDA_TRY(cudaMallocHost(&H->hscal, sizeof(double) * S_COUNT));
         H->mg.create(H->w, H->h, (int)cfg.mg_pre, (int)cfg.mg_post);
+        H->mg.omega = cfg.mg_omega > 0.0 ? (float)cfg.mg_omega : 1.0f;
+        H->inner_floor = cfg.inner_tol > 0.0 ? cfg.inner_tol : 1e-5;
+        SR_REQUIRE((size_t)div_up(H->w, 64) * div_up(H->h, 32) <= (size_t)PART_CAP, "world too large for the sums");
         (void)s;
     } catch (...) {
         heat_destroy(H);
@@ -721,12 +763,16 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
 
 void heat_destroy(HeatSolver* H) {
     if (!H) return;
+    for (auto& row : H->graphs)
+        for (auto& g : row)
+            if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(H->gas);
-    double* d64[] = {H->t0, H->C, H->t, H->u, H->ksum, H->kvac, H->diag, H->rhs, H->x, H->r64, H->lscale, H->kx, H->ky};
+    double* d64[] = {H->t0, H->C, H->t, H->u, H->ksum, H->kvac, H->c64, H->rhs, H->x, H->r64, H->lscale, H->kx, H->ky};
     for (double* p : d64) cudaFree(p);
     float* d32[] = {H->kap, H->sig, H->r32, H->e32, H->p32, H->q32, H->z32, H->fx, H->fy};
     for (float* p : d32) cudaFree(p);
     cudaFree(H->part);
+    cudaFree(H->counter);
     cudaFree(H->scal);
     if (H->hscal) cudaFreeHost(H->hscal);
     H->mg.destroy();
@@ -755,7 +801,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     R.precond = H->precond;
     setup_step(H, U, kappa, s);
     SR_CUDA_TRY(cudaMemcpyAsync(H->scal + S_DT, dt_dev, sizeof(double), cudaMemcpyDeviceToDevice, s));
-    H->read(S_NGAS, 3, s);  // gas cells, Δt, Σ C T⁰
+    H->read(S_HEAT0, 3, s);  // Σ C T⁰, gas cells, Δt
     H->n_gas = (int)H->hscal[S_NGAS];
     const double dt = H->hscal[S_DT];
     const double heat0 = H->hscal[S_HEAT0];
@@ -763,7 +809,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     if (H->cfg.pin_temperature || H->n_gas == 0 || !(dt > 0.0)) {
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx,
                                                                H->fy);
-    sr_note_launch();
+        sr_note_launch();
         *rep = R;
         rep->converged = 1;
         return;
@@ -774,16 +820,14 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     while (passes < H->max_passes && rounds < H->max_rounds) {
         passes++;
         build_system(H, dt, s);
-        SolveResult S = solve_pass(H, H->precond, H->cfg.solve_tol, (int)(H->max_rounds - rounds), s);
+        SolveResult S = solve_pass(H, H->precond, H->cfg.solve_tol, (int)(H->max_rounds - rounds), dt, s);
         rounds += (uint32_t)S.rounds;
         R.refinements += (uint32_t)S.refinements;
         R.rel_residual = S.rel;
         if (!S.ok) break;
         newton_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->cfg.newton_cell, H->gas, H->C, H->x, H->t, H->u,
-                                                              H->P(S_MOVED), H->P(S_VIOL));
-    sr_note_launch();
-        H->finalize(S_MOVED, H->grid, s);
-        H->finalize(S_VIOL, H->grid, s);
+                                                              H->red(S_MOVED));
+        sr_note_launch();
         H->read(S_MOVED, 2, s);
         if (H->hscal[S_MOVED] <= H->cfg.newton_heat * heat0 && H->hscal[S_VIOL] == 0.0) {
             converged = true;
@@ -794,32 +838,28 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     R.rounds = rounds;
     if (converged) {
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx, H->fy);
-    sr_note_launch();
+        sr_note_launch();
         commit_sums_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->t0, H->u, H->kvac,
-                                                           H->P(S_RAD), H->P(S_GAIN), H->P(S_HELD));
-    sr_note_launch();
-        H->finalize(S_RAD, H->grid, s);
-        H->finalize(S_GAIN, H->grid, s);
-        H->finalize(S_HELD, H->grid, s);
+                                                           H->red(S_RAD));
+        sr_note_launch();
         H->read(S_RAD, 3, s);
         const double rad = H->hscal[S_RAD], gain = H->hscal[S_GAIN], held = H->hscal[S_HELD];
         const double delta = -(gain + rad) / held;
         commit_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, delta, H->gas, H->C, H->t, H->t0, U);
-    sr_note_launch();
+        sr_note_launch();
         R.converged = 1;
         R.delta = delta;
         R.radiated = rad;
     } else {
         limited_scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->C, H->t0,
                                                              H->lscale);
-    sr_note_launch();
+        sr_note_launch();
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, H->lscale, H->fx,
                                                                H->fy);
-    sr_note_launch();
+        sr_note_launch();
         limited_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->lscale, U,
-                                                             H->P(S_RAD));
-    sr_note_launch();
-        H->finalize(S_RAD, H->grid, s);
+                                                             H->red(S_RAD));
+        sr_note_launch();
         H->read(S_RAD, 1, s);
         R.converged = 0;
         R.delta = 0.0;
@@ -833,14 +873,14 @@ void heat_first_solve(HeatSolver* H, const float* U, const float* kappa, double 
                       double* ms, uint32_t* rounds, double* rel_residual, double* x) {
     if (precond == SR_PRECOND_LEARNED) throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not loaded"};
     setup_step(H, U, kappa, s);
-    H->read(S_NGAS, 1, s);
+    H->read(S_HEAT0, 2, s);
     H->n_gas = (int)H->hscal[S_NGAS];
     build_system(H, dt, s);
     cudaEvent_t a, b;
     SR_CUDA_TRY(cudaEventCreate(&a));
     SR_CUDA_TRY(cudaEventCreate(&b));
     SR_CUDA_TRY(cudaEventRecord(a, s));
-    SolveResult S = solve_pass(H, precond, H->cfg.solve_tol, (int)H->max_rounds, s);
+    SolveResult S = solve_pass(H, precond, H->cfg.solve_tol, (int)H->max_rounds, dt, s);
     SR_CUDA_TRY(cudaEventRecord(b, s));
     SR_CUDA_TRY(cudaEventSynchronize(b));
     float t = 0.0f;

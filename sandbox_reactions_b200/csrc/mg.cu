@@ -2,18 +2,20 @@
 #include <vector>
 
 #include "mg.cuh"
+#include "reduce.cuh"
 
 namespace {
 
-constexpr int SX = 64, SY = 32;  // smoother tile (outputs)
+constexpr int SX = 64, SY = 32;  // smoother tile (outputs); even, so a tile's 2x2 aggregates stay inside it
 constexpr int SMOOTH_THREADS = 512;
 constexpr int TAIL_THREADS = 1024;
 
 struct TailArgs {
     int t, nl, pre, post;
     float omega;
+    const float* coarse_inv;  // the coarsest level's inverse, n x n
+    double* out;              // non-null when the tail's top level is level 0: <b, x2> written here
     MgLevel L[kMgMaxLevels];
-    double* part;  // non-null when the tail's top level is level 0: partials of <b, x2>
 };
 
 // Level 0's couplings to the +x / +y neighbours from the f64 faces, zero unless both cells are gas.
@@ -30,7 +32,8 @@ __global__ void mg_couplings0_kernel(MgLevel L, const double* __restrict__ kx, c
     }
 }
 
-// Level l+1 from level l: Galerkin aggregation of 2x2 cells (mg.cuh).
+// Level l+1 from level l: Galerkin aggregation of 2x2 cells (mg.cuh). The mass term c sums over the aggregate's
+// system cells; a coarse coupling sums the two fine couplings across the aggregates' shared side.
 __global__ void mg_coarsen_kernel(MgLevel F, MgLevel C) {
     const int wc = C.w, hc = C.h, wf = F.w, hf = F.h;
     const size_t nc = (size_t)wc * hc;
@@ -67,24 +70,27 @@ __global__ void mg_coarsen_kernel(MgLevel F, MgLevel C) {
     }
 }
 
-// One smoother on a big level: all NS half-sweeps of a tile in shared memory. PRE: from x = 0, red first, into L.x.
-// POST: from x = L.x + ω P xc (xc the coarse level's result), black first, into L.x2; `part` gets <b, x2> per CTA.
+// One smoother on a big level, all NS half-sweeps of a tile in shared memory (the tile's halo as deep as the
+// half-sweeps, so the tile's result is exactly the global red-black sweeps'). PRE: from x = 0, red first, into L.x,
+// then the residual summed over each 2x2 aggregate into the coarse level's b (one more halo ring keeps the residual's
+// neighbours exact). POST: from x = L.x + ω P xc, black first, into L.x2; at level 0 `out` gets <b, x2>.
 template <int NS, bool PRE>
-__global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, const float* __restrict__ xc, int wc,
-                                                                    float omega, double* part) {
-    constexpr int H = NS;
+__global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, MgLevel C, const float* __restrict__ xc,
+                                                                    float omega, double* part, unsigned* counter,
+                                                                    double* out) {
+    constexpr int H = PRE ? NS + 1 : NS;
     constexpr int RX = SX + 2 * H, RY = SY + 2 * H, RN = RX * RY;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float* sx = reinterpret_cast<float*>(smem_raw);
     float* sb = sx + RN;
     float* sdx = sb + RN;
     float* sdy = sdx + RN;
-    float* sinv = sdy + RN;
+    float* sc = sdy + RN;
+    float* sinv = sc + RN;
     uint8_t* sm = reinterpret_cast<uint8_t*>(sinv + RN);
     const int w = L.w, h = L.h;
     const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * SY - H;
     const int tid = threadIdx.x;
-    float* sc = sinv;  // c staged in the inverse-diagonal slot, replaced below
     for (int k = tid; k < RN; k += SMOOTH_THREADS) {
         const int lx = k % RX, ly = k / RX;
         const int gx = X0 + lx, gy = Y0 + ly;
@@ -99,7 +105,7 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, co
             m = L.mask[i];
             if (!PRE) {
                 x = L.x[i];
-                if (m) x += omega * xc[(size_t)(gy >> 1) * wc + (gx >> 1)];
+                if (m) x += omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
             }
         }
         sx[k] = x;
@@ -110,23 +116,11 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, co
         sm[k] = m;
     }
     __syncthreads();
-    // inverse diagonals of the interior (ring 0 is never updated)
-    float inv_local[(RN + SMOOTH_THREADS - 1) / SMOOTH_THREADS];
-#pragma unroll
-    for (int q = 0; q < (RN + SMOOTH_THREADS - 1) / SMOOTH_THREADS; q++) {
-        const int k = tid + q * SMOOTH_THREADS;
-        inv_local[q] = 0.0f;
-        if (k < RN) {
-            const int lx = k % RX, ly = k / RX;
-            if (lx > 0 && ly > 0 && lx < RX - 1 && ly < RY - 1)
-                inv_local[q] = 1.0f / (sc[k] + sdx[k] + sdx[k - 1] + sdy[k] + sdy[k - RX]);
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < (RN + SMOOTH_THREADS - 1) / SMOOTH_THREADS; q++) {
-        const int k = tid + q * SMOOTH_THREADS;
-        if (k < RN) sinv[k] = inv_local[q];
+    for (int k = tid; k < RN; k += SMOOTH_THREADS) {
+        const int lx = k % RX, ly = k / RX;
+        sinv[k] = (lx > 0 && ly > 0 && lx < RX - 1 && ly < RY - 1)
+                      ? 1.0f / (sc[k] + sdx[k] + sdx[k - 1] + sdy[k] + sdy[k - RX])
+                      : 0.0f;
     }
     __syncthreads();
     constexpr int HALF = RX / 2;
@@ -145,54 +139,87 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, co
         __syncthreads();
     }
     double acc = 0.0;
-    float* out = PRE ? L.x : L.x2;
+    float* dst = PRE ? L.x : L.x2;
     for (int k = tid; k < SX * SY; k += SMOOTH_THREADS) {
         const int ox = k % SX, oy = k / SX;
         const int gx = X0 + H + ox, gy = Y0 + H + oy;
         if (gx < w && gy < h) {
             const int l = (oy + H) * RX + ox + H;
-            out[(size_t)gy * w + gx] = sx[l];
-            if (!PRE && part) acc += (double)sb[l] * (double)sx[l];
+            dst[(size_t)gy * w + gx] = sx[l];
+            if (!PRE && out) acc += (double)sb[l] * (double)sx[l];
         }
     }
-    if (!PRE && part) {
-        __shared__ double red[SMOOTH_THREADS / 32];
+    if (PRE) {
+        // the coarse right-hand side: the residual, in difference form, summed over each aggregate of the tile
+        for (int k = tid; k < (SX / 2) * (SY / 2); k += SMOOTH_THREADS) {
+            const int cxl = k % (SX / 2), cyl = k / (SX / 2);
+            const int X = (X0 + H) / 2 + cxl, Y = (Y0 + H) / 2 + cyl;
+            if (X >= C.w || Y >= C.h) continue;
+            float sum = 0.0f;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if ((tid & 31) == 0) red[tid >> 5] = acc;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int q = 0; q < SMOOTH_THREADS / 32; q++) t += red[q];
-            part[blockIdx.y * gridDim.x + blockIdx.x] = t;
+            for (int b = 0; b < 2; b++)
+#pragma unroll
+                for (int a = 0; a < 2; a++) {
+                    const int gx = 2 * X + a, gy = 2 * Y + b;
+                    if (gx >= w || gy >= h) continue;
+                    const int l = (2 * cyl + b + H) * RX + 2 * cxl + a + H;
+                    if (!sm[l]) continue;
+                    const float xj = sx[l];
+                    float ax = sc[l] * xj;
+                    ax += sdx[l - 1] * (xj - sx[l - 1]);
+                    ax += sdx[l] * (xj - sx[l + 1]);
+                    ax += sdy[l - RX] * (xj - sx[l - RX]);
+                    ax += sdy[l] * (xj - sx[l + RX]);
+                    sum += sb[l] - ax;
+                }
+            C.b[(size_t)Y * C.w + X] = C.mask[(size_t)Y * C.w + X] ? sum : 0.0f;
         }
+    } else if (out) {
+        grid_sum_last1(acc, part, counter, out);
     }
 }
 
-// The residual of the pre-smoothed level summed over each 2x2 aggregate: the coarse right-hand side.
-__global__ void mg_restrict_kernel(MgLevel F, MgLevel C) {
-    const int wc = C.w, hc = C.h, wf = F.w, hf = F.h;
-    const size_t nc = (size_t)wc * hc;
-    for (size_t I = (size_t)blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += (size_t)gridDim.x * blockDim.x) {
-        const int X = (int)(I % wc), Y = (int)(I / wc);
-        float sum = 0.0f;
-#pragma unroll
-        for (int b = 0; b < 2; b++)
-#pragma unroll
-            for (int a = 0; a < 2; a++) {
-                const int x = 2 * X + a, y = 2 * Y + b;
-                if (x >= wf || y >= hf) continue;
-                const size_t j = (size_t)y * wf + x;
-                if (!F.mask[j]) continue;
-                const float xl = x > 0 ? F.x[j - 1] : 0.0f, xr = x + 1 < wf ? F.x[j + 1] : 0.0f;
-                const float xu = y > 0 ? F.x[j - wf] : 0.0f, xd = y + 1 < hf ? F.x[j + wf] : 0.0f;
-                const float dl = x > 0 ? F.dx[j - 1] : 0.0f, du = y > 0 ? F.dy[j - wf] : 0.0f;
-                const float dr = F.dx[j], dd = F.dy[j];
-                const float diag = F.c[j] + dl + dr + du + dd;
-                sum += F.b[j] - (diag * F.x[j] - dl * xl - dr * xr - du * xu - dd * xd);
-            }
-        C.b[I] = C.mask[I] ? sum : 0.0f;
+// The coarsest level's operator inverted by Gauss-Jordan elimination in f64 in one CTA (n <= 64 cells), masked-out
+// cells as identity rows; stored f32. The operator is SPD and diagonally dominant, so no pivoting is needed.
+__global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
+    extern __shared__ double aug[];  // n x 2n
+    const int w = C.w, h = C.h, n = w * h, m = 2 * n;
+    for (int k = threadIdx.x; k < n * m; k += blockDim.x) {
+        const int i = k / m, j = k % m;
+        double v = 0.0;
+        if (j >= n) {
+            v = (j - n == i) ? 1.0 : 0.0;
+        } else if (!C.mask[i]) {
+            v = (i == j) ? 1.0 : 0.0;
+        } else {
+            const int xi = i % w, yi = i / w;
+            const double dl = xi > 0 ? C.dx[i - 1] : 0.0, dr = C.dx[i];
+            const double du = yi > 0 ? C.dy[i - w] : 0.0, dd = C.dy[i];
+            if (j == i) v = (double)C.c[i] + dl + dr + du + dd;
+            else if (xi > 0 && j == i - 1) v = -dl;
+            else if (xi + 1 < w && j == i + 1) v = -dr;
+            else if (yi > 0 && j == i - w) v = -du;
+            else if (yi + 1 < h && j == i + w) v = -dd;
+        }
+        aug[k] = v;
     }
+    __syncthreads();
+    for (int p = 0; p < n; p++) {
+        const double piv = aug[p * m + p];
+        __syncthreads();
+        for (int j = threadIdx.x; j < m; j += blockDim.x) aug[p * m + j] /= piv;
+        __syncthreads();
+        for (int k = threadIdx.x; k < n * m; k += blockDim.x) {
+            const int i = k / m, j = k % m;
+            if (i != p && j != p) aug[k] -= aug[i * m + p] * aug[p * m + j];
+        }
+        __syncthreads();
+        // column p of the other rows, read as the elimination factor above, becomes 0
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            if (i != p) aug[i * m + p] = 0.0;
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) inv[k] = (float)aug[(k / n) * m + n + (k % n)];
 }
 
 // ---- the coarse tail: every level from t on, inside one CTA
@@ -230,11 +257,13 @@ __device__ void tail_restrict(const TailLevel& F, const TailLevel& C) {
                 if (x >= F.w || y >= F.h) continue;
                 const int j = y * F.w + x;
                 if (!F.m[j]) continue;
-                const float xl = x > 0 ? F.x[j - 1] : 0.0f, xr = x + 1 < F.w ? F.x[j + 1] : 0.0f;
-                const float xu = y > 0 ? F.x[j - F.w] : 0.0f, xd = y + 1 < F.h ? F.x[j + F.w] : 0.0f;
-                const float dl = x > 0 ? F.dx[j - 1] : 0.0f, du = y > 0 ? F.dy[j - F.w] : 0.0f;
-                const float dr = F.dx[j], dd = F.dy[j];
-                sum += F.b[j] - ((F.c[j] + dl + dr + du + dd) * F.x[j] - dl * xl - dr * xr - du * xu - dd * xd);
+                const float xj = F.x[j];
+                float ax = F.c[j] * xj;
+                if (x > 0) ax += F.dx[j - 1] * (xj - F.x[j - 1]);
+                if (x + 1 < F.w) ax += F.dx[j] * (xj - F.x[j + 1]);
+                if (y > 0) ax += F.dy[j - F.w] * (xj - F.x[j - F.w]);
+                if (y + 1 < F.h) ax += F.dy[j] * (xj - F.x[j + F.w]);
+                sum += F.b[j] - ax;
             }
         C.b[I] = C.m[I] ? sum : 0.0f;
         C.x[I] = 0.0f;
@@ -283,20 +312,23 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
         tail_restrict(T[l], T[l + 1]);
     }
     {
-        const TailLevel& C = T[A.nl - 1];
-        tail_sweep(C, 0);
-        for (int s = 0; s < kMgCoarsestSweeps; s++) {
-            tail_sweep(C, 1);
-            tail_sweep(C, 0);
+        // the coarsest level exactly: x = A⁻¹ b with the inverse built once per Newton pass (mg_coarse_inverse_kernel)
+        const TailLevel& Cs = T[A.nl - 1];
+        const int n = Cs.w * Cs.h;
+        for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
+            float s = 0.0f;
+            for (int k = 0; k < n; k++) s += A.coarse_inv[i * n + k] * Cs.b[k];
+            Cs.x[i] = Cs.m[i] ? s : 0.0f;
         }
+        __syncthreads();
     }
     for (int l = A.nl - 2; l >= A.t; l--) {
         const TailLevel& F = T[l];
-        const TailLevel& C = T[l + 1];
+        const TailLevel& Cs = T[l + 1];
         const int n = F.w * F.h;
         for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
             const int x = i % F.w, y = i / F.w;
-            if (F.m[i]) F.x[i] += A.omega * C.x[(y >> 1) * C.w + (x >> 1)];
+            if (F.m[i]) F.x[i] += A.omega * Cs.x[(y >> 1) * Cs.w + (x >> 1)];
         }
         __syncthreads();
         for (int s = 0; s < A.post; s++) {
@@ -311,7 +343,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
         A.L[A.t].x2[i] = top.x[i];
         acc += (double)top.b[i] * (double)top.x[i];
     }
-    if (A.part) {
+    if (A.out) {
         __shared__ double red[TAIL_THREADS / 32];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -320,7 +352,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
         if (threadIdx.x == 0) {
             double t = 0.0;
             for (int q = 0; q < TAIL_THREADS / 32; q++) t += red[q];
-            A.part[0] = t;
+            *A.out = t;
         }
     }
 }
@@ -331,31 +363,41 @@ size_t tail_smem(const Multigrid& M) {
     return (s + 15) & ~(size_t)15;
 }
 
-template <int NS>
-size_t smooth_smem() {
-    constexpr int RN = (SX + 2 * NS) * (SY + 2 * NS);
-    return (size_t)RN * (5 * sizeof(float) + 1);
+template <int NS, bool PRE>
+constexpr size_t smooth_smem() {
+    constexpr int H = PRE ? NS + 1 : NS;
+    constexpr int RN = (SX + 2 * H) * (SY + 2 * H);
+    return (size_t)RN * (6 * sizeof(float) + 1);
 }
 
 template <int NS, bool PRE>
-void launch_smooth(const MgLevel& L, const float* xc, int wc, float omega, double* part, cudaStream_t s) {
-    size_t smem = smooth_smem<NS>();
-    cudaFuncSetAttribute(mg_smooth_kernel<NS, PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+void launch_smooth(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
+                   double* out, cudaStream_t s) {
     dim3 grid(div_up(L.w, SX), div_up(L.h, SY));
-    mg_smooth_kernel<NS, PRE><<<grid, SMOOTH_THREADS, smem, s>>>(L, xc, wc, omega, part);
+    mg_smooth_kernel<NS, PRE><<<grid, SMOOTH_THREADS, smooth_smem<NS, PRE>(), s>>>(L, C, xc, omega, part, counter,
+                                                                                    out);
     sr_note_launch();
 }
 
-void smooth(int nu, bool pre, const MgLevel& L, const float* xc, int wc, float omega, double* part, cudaStream_t s) {
+void smooth(int nu, bool pre, const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part,
+            unsigned* counter, double* out, cudaStream_t s) {
     if (pre) {
-        if (nu == 1) launch_smooth<2, true>(L, xc, wc, omega, part, s);
-        else if (nu == 2) launch_smooth<4, true>(L, xc, wc, omega, part, s);
-        else launch_smooth<6, true>(L, xc, wc, omega, part, s);
+        if (nu == 1) launch_smooth<2, true>(L, C, xc, omega, part, counter, out, s);
+        else if (nu == 2) launch_smooth<4, true>(L, C, xc, omega, part, counter, out, s);
+        else launch_smooth<6, true>(L, C, xc, omega, part, counter, out, s);
     } else {
-        if (nu == 1) launch_smooth<2, false>(L, xc, wc, omega, part, s);
-        else if (nu == 2) launch_smooth<4, false>(L, xc, wc, omega, part, s);
-        else launch_smooth<6, false>(L, xc, wc, omega, part, s);
+        if (nu == 1) launch_smooth<2, false>(L, C, xc, omega, part, counter, out, s);
+        else if (nu == 2) launch_smooth<4, false>(L, C, xc, omega, part, counter, out, s);
+        else launch_smooth<6, false>(L, C, xc, omega, part, counter, out, s);
     }
+}
+
+template <int NS>
+void set_attributes_ns() {
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smooth_smem<NS, true>()));
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smooth_smem<NS, false>()));
 }
 
 int grid_for(size_t n) {
@@ -392,11 +434,17 @@ void Multigrid::create(int w, int h, int pre_, int post_) {
     }
     tail = 0;
     while ((size_t)L[tail].w * L[tail].h > (size_t)kMgTailCells) tail++;
-    part_count = tail == 0 ? 1 : (int)(div_up(w, SX) * div_up(h, SY));
-    SR_CUDA_TRY(cudaMalloc(&part, sizeof(double) * part_count));
     size_t ts = tail_smem(*this);
     SR_REQUIRE(ts <= 200 * 1024, "the coarse tail does not fit in shared memory");
     SR_CUDA_TRY(cudaFuncSetAttribute(mg_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ts));
+    const size_t nc = (size_t)L[nlevels - 1].w * L[nlevels - 1].h;
+    SR_REQUIRE(nc <= 64, "the coarsest level holds more than 64 cells");
+    SR_CUDA_TRY(cudaMalloc(&coarse_inv, sizeof(float) * nc * nc));
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(nc * 2 * nc * sizeof(double))));
+    set_attributes_ns<2>();
+    set_attributes_ns<4>();
+    set_attributes_ns<6>();
 }
 
 void Multigrid::destroy() {
@@ -412,8 +460,8 @@ void Multigrid::destroy() {
         }
         L[l] = MgLevel();
     }
-    cudaFree(part);
-    part = nullptr;
+    cudaFree(coarse_inv);
+    coarse_inv = nullptr;
     nlevels = 0;
 }
 
@@ -429,29 +477,32 @@ void Multigrid::set_couplings(const double* kx, const double* ky, const uint8_t*
 }
 
 void Multigrid::coarsen(cudaStream_t s) {
-    for (int l = 1; l < nlevels; l++)
+    for (int l = 1; l < nlevels; l++) {
         mg_coarsen_kernel<<<grid_for((size_t)L[l].w * L[l].h), 256, 0, s>>>(L[l - 1], L[l]);
+        sr_note_launch();
+    }
+    const MgLevel& C = L[nlevels - 1];
+    const size_t nc = (size_t)C.w * C.h;
+    mg_coarse_inverse_kernel<<<1, 512, nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
     sr_note_launch();
 }
 
-void Multigrid::apply(const float* r, float* z, cudaStream_t s) {
+void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter, double* rz_out, cudaStream_t s) {
     L[0].b = const_cast<float*>(r);
     L[0].x2 = z;
-    for (int l = 0; l < tail; l++) {
-        smooth(pre, true, L[l], nullptr, 0, omega, nullptr, s);
-        mg_restrict_kernel<<<grid_for((size_t)L[l + 1].w * L[l + 1].h), 256, 0, s>>>(L[l], L[l + 1]);
-    sr_note_launch();
-    }
+    for (int l = 0; l < tail; l++) smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s);
     TailArgs T;
+    T.coarse_inv = coarse_inv;
     T.t = tail;
     T.nl = nlevels;
     T.pre = pre;
     T.post = post;
     T.omega = omega;
+    T.out = tail == 0 ? rz_out : nullptr;
     for (int l = 0; l < nlevels; l++) T.L[l] = L[l];
-    T.part = tail == 0 ? part : nullptr;
     mg_tail_kernel<<<1, TAIL_THREADS, tail_smem(*this), s>>>(T);
     sr_note_launch();
     for (int l = tail - 1; l >= 0; l--)
-        smooth(post, false, L[l], L[l + 1].x2, L[l + 1].w, omega, l == 0 ? part : nullptr, s);
+        smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, l == 0 ? part : nullptr, l == 0 ? counter : nullptr,
+               l == 0 ? rz_out : nullptr, s);
 }

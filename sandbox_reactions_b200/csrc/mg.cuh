@@ -7,13 +7,13 @@
 // crates/sr-engine/shaders/heat.wgsl:1315-1398). Smoothing is red-black Gauss-Seidel (global parity), V(pre, post),
 // the post-smoother sweeping the colours in reverse so the cycle is symmetric. Big levels run as tile kernels that do
 // all of a smoother's half-sweeps in shared memory (temporal blocking: the tile's halo is as deep as the half-sweeps);
-// every level of at most kMgTailCells cells runs inside one CTA (the coarse tail, the reference's mg_coarse).
+// every level of at most kMgTailCells cells runs inside one CTA (the coarse tail, the reference's mg_coarse), and the
+// coarsest level (at most 8 x 8) is solved exactly by its inverse, built once per Newton pass.
 #pragma once
 
 #include "common.cuh"
 
 constexpr int kMgTailCells = 4096;   // levels at most this large are solved inside one CTA
-constexpr int kMgCoarsestSweeps = 40;  // symmetric red-black sweep pairs on the coarsest level
 constexpr int kMgMaxLevels = 16;
 
 struct MgLevel {
@@ -33,8 +33,7 @@ struct Multigrid {
     int pre = 2, post = 2;
     float omega = 1.0f;  // coarse-correction weight
     MgLevel L[kMgMaxLevels];
-    double* part = nullptr;  // per-CTA partials of <b, x> of the level-0 post-smoother
-    int part_count = 0;
+    float* coarse_inv = nullptr;  // the coarsest level's operator inverted (at most 64 x 64), per Newton pass
 
     void create(int w, int h, int pre, int post);
     void destroy();
@@ -43,6 +42,6 @@ struct Multigrid {
     void set_couplings(const double* kx, const double* ky, const uint8_t* gas, cudaStream_t s);
     // Every coarse level's operator, once level 0's c (written by the caller, per Newton pass) is in place.
     void coarsen(cudaStream_t s);
-    // z = M r (level-0 b := r, x := z); partials of <r, z> into `part` (part_count of them).
-    void apply(const float* r, float* z, cudaStream_t s);
+    // z = M r (level-0 b := r, x2 := z), and <r, z> into *rz_out (a one-launch grid sum over `part` and `counter`).
+    void apply(const float* r, float* z, double* part, unsigned* counter, double* rz_out, cudaStream_t s);
 };

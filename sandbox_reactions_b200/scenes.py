@@ -7,7 +7,8 @@ Seeds follow seed = 1000 + 100 * config + scene. Each generator returns (Config,
   - fld:        implicit FLD alone (config 3): κ lognormal with a 32-cell correlation length spanning six decades
                 (0.1-99.9 percentiles), T = 1e3 background with three hot spots at 1e6, Σ = 1, Δt = 50 x the
                 explicit diffusion limit;
-  - full_step:  the disk of config 2 with the opacity field of config 3 and hot spots, every pass on (the
+  - full_step:  the disk of config 2 with the opacity field of config 3 and hot spots at T = 100 over T = 1 (the
+                reference's burning temperatures are 56-135), every pass on (the
                 hydro+gravity+FLD step of the headline metric).
 """
 from __future__ import annotations
@@ -150,7 +151,7 @@ def _disk_fields(n, rng, sigma0):
     return sigma, u, v
 
 
-def full_step(n: int = 2048, scene: int = 0, sigma0: float = 1.0, t_bg: float = 1.0, t_spot: float = 1e3):
+def full_step(n: int = 2048, scene: int = 0, sigma0: float = 1.0, t_bg: float = 1.0, t_spot: float = 100.0):
     """Hydro + gravity + FLD on one world: config 2's disk, config 3's opacity field, hot spots in the gas."""
     rng = np.random.default_rng(seed_of(5, scene))
     gamma, mu = 5.0 / 3.0, 1.0
