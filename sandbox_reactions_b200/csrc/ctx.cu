@@ -339,6 +339,7 @@ sr_status sr_upload(sr_ctx* c, const float* p, uint32_t nplanes) {
         SR_REQUIRE(p, "sr_upload: null planes");
         SR_REQUIRE(nplanes == 4, "sr_upload: this build carries 4 planes");
         SR_CUDA_TRY(cudaMemcpyAsync(planes(c), p, sizeof(float) * 4 * c->n, cudaMemcpyHostToDevice, c->stream));
+        if (c->heat) heat_reset(c->heat, c->stream);
         initial_reductions(c);
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
         c->uploaded = true;

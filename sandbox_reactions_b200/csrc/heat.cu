@@ -438,13 +438,31 @@ __global__ void commit_sums_kernel(HeatConst K, double dt, const uint8_t* __rest
     grid_sum_last<3>(v, R.part, R.counter, R.out);
 }
 
-// E_i += C_i ((1 + δ) T_i - T_i⁰) (heat.rs:532-535).
-__global__ void commit_apply_kernel(HeatConst K, double delta, const uint8_t* __restrict__ gas,
+// E_i += C_i ((1 + δ) T_i - T_i⁰) (heat.rs:532-535), and the cell's rate (T - T⁰)/Δt kept for the next step's first
+// iterate (heat.wgsl:1139-1155).
+__global__ void commit_apply_kernel(HeatConst K, double delta, double dt, const uint8_t* __restrict__ gas,
                                     const double* __restrict__ C, const double* __restrict__ t,
-                                    const double* __restrict__ t0, float* U) {
+                                    const double* __restrict__ t0, float* U, double* rate) {
     const size_t n = (size_t)K.w * K.h;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (gas[i]) U[3 * n + i] = (float)((double)U[3 * n + i] + C[i] * ((1.0 + delta) * t[i] - t0[i]));
+        rate[i] = gas[i] ? (t[i] - t0[i]) / dt : 0.0;
+    }
+}
+
+// The first iterate on the V-cycle (heat.wgsl:710-722): T⁰ + the last step's rate × Δt, T⁰ where that is off by more
+// than a factor 2 or not finite, floored at T_floor.
+__global__ void warm_start_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+                                  const double* __restrict__ t0, const double* __restrict__ rate, double* t, double* u) {
+    const size_t n = (size_t)K.w * K.h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (!gas[i]) continue;
+        double tg = t0[i] + rate[i] * dt;
+        if (!(tg >= 0.5 * t0[i] && tg <= 2.0 * t0[i])) tg = t0[i];
+        tg = fmax(tg, K.t_floor);
+        t[i] = tg;
+        u[i] = u_of(K, tg);
+    }
 }
 
 // Past the ceiling (heat.rs:545-564): each gas cell's outflow scaled to the heat it holds above its floor.
@@ -537,6 +555,7 @@ struct HeatSolver {
     double *t0 = nullptr, *C = nullptr, *t = nullptr, *u = nullptr, *kx = nullptr, *ky = nullptr;
     double *ksum = nullptr, *kvac = nullptr, *c64 = nullptr, *rhs = nullptr, *x = nullptr, *r64 = nullptr;
     double* lscale = nullptr;
+    double* rate = nullptr;      // each cell's P5 rate (T - T⁰)/Δt in the last step, for the next first iterate
     float *kap = nullptr, *sig = nullptr;
     float *r32 = nullptr, *e32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr;
     float *fx = nullptr, *fy = nullptr;
@@ -733,8 +752,9 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         const size_t n = H->n, nx = (size_t)(H->w + 1) * H->h, ny = (size_t)H->w * (H->h + 1);
         SR_CUDA_TRY(cudaMalloc(&H->gas, n));
         double** d64[] = {&H->t0, &H->C, &H->t, &H->u, &H->ksum, &H->kvac, &H->c64, &H->rhs, &H->x, &H->r64,
-                          &H->lscale};
+                          &H->lscale, &H->rate};
         for (double** p : d64) SR_CUDA_TRY(cudaMalloc(p, sizeof(double) * n));
+        SR_CUDA_TRY(cudaMemset(H->rate, 0, sizeof(double) * n));
         SR_CUDA_TRY(cudaMalloc(&H->kx, sizeof(double) * nx));
         SR_CUDA_TRY(cudaMalloc(&H->ky, sizeof(double) * ny));
         float** d32[] = {&H->kap, &H->sig, &H->r32, &H->e32, &H->p32, &H->q32, &H->z32};
@@ -767,7 +787,8 @@ void heat_destroy(HeatSolver* H) {
         for (auto& g : row)
             if (g.exec) cudaGraphExecDestroy(g.exec);
     cudaFree(H->gas);
-    double* d64[] = {H->t0, H->C, H->t, H->u, H->ksum, H->kvac, H->c64, H->rhs, H->x, H->r64, H->lscale, H->kx, H->ky};
+    double* d64[] = {H->t0, H->C, H->t, H->u, H->ksum, H->kvac, H->c64, H->rhs, H->x, H->r64, H->lscale, H->rate,
+                     H->kx, H->ky};
     for (double* p : d64) cudaFree(p);
     float* d32[] = {H->kap, H->sig, H->r32, H->e32, H->p32, H->q32, H->z32, H->fx, H->fy};
     for (float* p : d32) cudaFree(p);
@@ -783,6 +804,8 @@ void heat_set_precond(HeatSolver* H, uint32_t precond) {
     if (precond == SR_PRECOND_LEARNED) throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not loaded"};
     H->precond = precond;
 }
+
+void heat_reset(HeatSolver* H, cudaStream_t s) { SR_CUDA_TRY(cudaMemsetAsync(H->rate, 0, sizeof(double) * H->n, s)); }
 
 void heat_set_limits(HeatSolver* H, uint32_t max_passes, uint32_t max_rounds) {
     H->max_passes = max_passes;
@@ -815,12 +838,20 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         return;
     }
     R.dt = dt;
+    if (H->precond != SR_PRECOND_JACOBI) {
+        warm_start_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->t0, H->rate, H->t, H->u);
+        sr_note_launch();
+    }
     uint32_t passes = 0, rounds = 0;
     bool converged = false;
+    // Inexact Newton: a pass's solve is asked for 1e-2 of the last pass's relative heat moved (at most 1e-4), never
+    // less than solve_tol; the passes end only on a pass solved to solve_tol.
+    const double tol = H->cfg.solve_tol;
+    double pass_tol = std::max(tol, 1e-4);
     while (passes < H->max_passes && rounds < H->max_rounds) {
         passes++;
         build_system(H, dt, s);
-        SolveResult S = solve_pass(H, H->precond, H->cfg.solve_tol, (int)(H->max_rounds - rounds), dt, s);
+        SolveResult S = solve_pass(H, H->precond, pass_tol, (int)(H->max_rounds - rounds), dt, s);
         rounds += (uint32_t)S.rounds;
         R.refinements += (uint32_t)S.refinements;
         R.rel_residual = S.rel;
@@ -829,10 +860,12 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
                                                               H->red(S_MOVED));
         sr_note_launch();
         H->read(S_MOVED, 2, s);
-        if (H->hscal[S_MOVED] <= H->cfg.newton_heat * heat0 && H->hscal[S_VIOL] == 0.0) {
+        const double rel_moved = heat0 > 0.0 ? H->hscal[S_MOVED] / heat0 : 0.0;
+        if (rel_moved <= H->cfg.newton_heat && H->hscal[S_VIOL] == 0.0 && pass_tol <= tol) {
             converged = true;
             break;
         }
+        pass_tol = std::max(tol, std::min(1e-4, 1e-2 * rel_moved));
     }
     R.passes = passes;
     R.rounds = rounds;
@@ -845,7 +878,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         H->read(S_RAD, 3, s);
         const double rad = H->hscal[S_RAD], gain = H->hscal[S_GAIN], held = H->hscal[S_HELD];
         const double delta = -(gain + rad) / held;
-        commit_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, delta, H->gas, H->C, H->t, H->t0, U);
+        commit_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, delta, dt, H->gas, H->C, H->t, H->t0, U, H->rate);
         sr_note_launch();
         R.converged = 1;
         R.delta = delta;
@@ -860,6 +893,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         limited_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->lscale, U,
                                                              H->red(S_RAD));
         sr_note_launch();
+        SR_CUDA_TRY(cudaMemsetAsync(H->rate, 0, sizeof(double) * H->n, s));
         H->read(S_RAD, 1, s);
         R.converged = 0;
         R.delta = 0.0;

@@ -11,6 +11,8 @@ void heat_destroy(HeatSolver* hs);
 // One implicit step of length *dt_dev on the 4 planes U (E changes), κ from `kappa` (W*H) or cfg.kappa0.
 void heat_step(HeatSolver* hs, float* U, const float* kappa, const double* dt_dev, cudaStream_t s, sr_heat_report* rep);
 void heat_read_flux(HeatSolver* hs, float* fx, float* fy);
+// Forgets the last step's rates (a new state was uploaded).
+void heat_reset(HeatSolver* hs, cudaStream_t s);
 void heat_set_precond(HeatSolver* hs, uint32_t precond);
 void heat_set_limits(HeatSolver* hs, uint32_t max_passes, uint32_t max_rounds);
 // The first Newton pass's system of a step of length dt, solved alone (timed on the device).

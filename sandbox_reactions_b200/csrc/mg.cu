@@ -229,45 +229,51 @@ struct TailLevel {
     uint8_t* m;
 };
 
+// Threads of the tail run as 32 x 32: thread (tx, ty) takes rows ty, ty + 32, ... and, of a sweep's colour, the
+// columns 2 tx + parity, 2 (tx + 32) + parity, ... (no index divisions).
 __device__ void tail_sweep(const TailLevel& T, int color) {
-    const int n = T.w * T.h;
-    for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
-        const int x = i % T.w, y = i / T.w;
-        if (((x + y) & 1) != color || !T.m[i]) continue;
-        const float dl = x > 0 ? T.dx[i - 1] : 0.0f, du = y > 0 ? T.dy[i - T.w] : 0.0f;
-        const float dr = T.dx[i], dd = T.dy[i];
-        float s = T.b[i];
-        if (x > 0) s += dl * T.x[i - 1];
-        if (x + 1 < T.w) s += dr * T.x[i + 1];
-        if (y > 0) s += du * T.x[i - T.w];
-        if (y + 1 < T.h) s += dd * T.x[i + T.w];
-        T.x[i] = s / (T.c[i] + dl + dr + du + dd);
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int y = ty; y < T.h; y += 32) {
+        const int par = (y + color) & 1;
+        for (int x = 2 * tx + par; x < T.w; x += 64) {
+            const int i = y * T.w + x;
+            if (!T.m[i]) continue;
+            const float dl = x > 0 ? T.dx[i - 1] : 0.0f, du = y > 0 ? T.dy[i - T.w] : 0.0f;
+            const float dr = T.dx[i], dd = T.dy[i];
+            float s = T.b[i];
+            if (x > 0) s += dl * T.x[i - 1];
+            if (x + 1 < T.w) s += dr * T.x[i + 1];
+            if (y > 0) s += du * T.x[i - T.w];
+            if (y + 1 < T.h) s += dd * T.x[i + T.w];
+            T.x[i] = s / (T.c[i] + dl + dr + du + dd);
+        }
     }
     __syncthreads();
 }
 
 __device__ void tail_restrict(const TailLevel& F, const TailLevel& C) {
-    const int nc = C.w * C.h;
-    for (int I = threadIdx.x; I < nc; I += TAIL_THREADS) {
-        const int X = I % C.w, Y = I / C.w;
-        float sum = 0.0f;
-        for (int b = 0; b < 2; b++)
-            for (int a = 0; a < 2; a++) {
-                const int x = 2 * X + a, y = 2 * Y + b;
-                if (x >= F.w || y >= F.h) continue;
-                const int j = y * F.w + x;
-                if (!F.m[j]) continue;
-                const float xj = F.x[j];
-                float ax = F.c[j] * xj;
-                if (x > 0) ax += F.dx[j - 1] * (xj - F.x[j - 1]);
-                if (x + 1 < F.w) ax += F.dx[j] * (xj - F.x[j + 1]);
-                if (y > 0) ax += F.dy[j - F.w] * (xj - F.x[j - F.w]);
-                if (y + 1 < F.h) ax += F.dy[j] * (xj - F.x[j + F.w]);
-                sum += F.b[j] - ax;
-            }
-        C.b[I] = C.m[I] ? sum : 0.0f;
-        C.x[I] = 0.0f;
-    }
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int Y = ty; Y < C.h; Y += 32)
+        for (int X = tx; X < C.w; X += 32) {
+            const int I = Y * C.w + X;
+            float sum = 0.0f;
+            for (int b = 0; b < 2; b++)
+                for (int a = 0; a < 2; a++) {
+                    const int x = 2 * X + a, y = 2 * Y + b;
+                    if (x >= F.w || y >= F.h) continue;
+                    const int j = y * F.w + x;
+                    if (!F.m[j]) continue;
+                    const float xj = F.x[j];
+                    float ax = F.c[j] * xj;
+                    if (x > 0) ax += F.dx[j - 1] * (xj - F.x[j - 1]);
+                    if (x + 1 < F.w) ax += F.dx[j] * (xj - F.x[j + 1]);
+                    if (y > 0) ax += F.dy[j - F.w] * (xj - F.x[j - F.w]);
+                    if (y + 1 < F.h) ax += F.dy[j] * (xj - F.x[j + F.w]);
+                    sum += F.b[j] - ax;
+                }
+            C.b[I] = C.m[I] ? sum : 0.0f;
+            C.x[I] = 0.0f;
+        }
     __syncthreads();
 }
 
@@ -326,9 +332,14 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
         const TailLevel& F = T[l];
         const TailLevel& Cs = T[l + 1];
         const int n = F.w * F.h;
-        for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
-            const int x = i % F.w, y = i / F.w;
-            if (F.m[i]) F.x[i] += A.omega * Cs.x[(y >> 1) * Cs.w + (x >> 1)];
+        (void)n;
+        {
+            const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+            for (int y = ty; y < F.h; y += 32)
+                for (int x = tx; x < F.w; x += 32) {
+                    const int i = y * F.w + x;
+                    if (F.m[i]) F.x[i] += A.omega * Cs.x[(y >> 1) * Cs.w + (x >> 1)];
+                }
         }
         __syncthreads();
         for (int s = 0; s < A.post; s++) {
