@@ -190,6 +190,18 @@ sr_status sr_read_cost(sr_ctx* ctx, sr_cost* out);
 sr_status sr_heat_first_solve(sr_ctx* ctx, double dt, uint32_t precond, double* ms, uint32_t* rounds,
                               double* rel_residual, double* x);
 
+/* P2's gravity solve (φ and g = -∇φ of Σ, as a context's) with no device allocation — no counterpart in the
+ * reference. For callers that cannot allocate device memory: hosts that own every byte of device memory and hand their
+ * plug-ins buffers (no cudaMalloc allowed), or loops that cannot afford cudaMalloc's device-wide synchronisation. The
+ * caller passes device buffers: `sigma` (W*H) in, `phi`, `gx`, `gy` (W*H each) out, and the CUDA stream (NULL: the
+ * default stream) as `stream`. The scratch lives in static device arrays sized for worlds up to 256 x 256 cells, held
+ * by every GPU that loads the library until exit; a larger world is refused with SR_E_INVALID. The first call on a
+ * device looks up the arrays and uploads the kernel's spectrum, so it should come before any stream capture. Calls
+ * share the arrays: calls whose work overlaps on the GPU race. Uses cfg's width, height, kernel, G, softening and
+ * sigma_vac. */
+sr_status sr_gravity_solve_static(const sr_config* cfg, const float* sigma, float* phi, float* gx, float* gy,
+                                  void* stream);
+
 /* The message of the last failed call on `ctx` (or of the last failed sr_create when ctx is NULL). */
 const char* sr_last_error(const sr_ctx* ctx);
 

@@ -111,6 +111,8 @@ SR_HOST_DEVICE void euler_flux(const Prim& p, float energy, int dir, float* f) {
 
 // ------------------------------------------------------------------------------------------------ launch helpers
 // Every kernel launch of the library is counted (sr_cost.kernel_launches reports the count of an sr_step call).
+// The message sr_last_error(NULL) returns (calls without a context).
+void sr_set_global_error(const std::string& message);
 void sr_note_launch();
 void sr_note_launches(long long n);
 unsigned long long sr_launches();

@@ -19,6 +19,7 @@ thread_local std::string g_create_error;
 std::atomic<unsigned long long> g_launches{0};
 }  // namespace
 
+void sr_set_global_error(const std::string& message) { g_create_error = message; }
 void sr_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void sr_note_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 unsigned long long sr_launches() { return g_launches.load(std::memory_order_relaxed); }

@@ -60,6 +60,9 @@ def load_library(path: str = LIB_PATH):
     L.sr_set_timing.argtypes = [P, C.c_int32]
     L.sr_read_cost.argtypes = [P, C.POINTER(sr_cost)]
     L.sr_heat_first_solve.argtypes = [P, C.c_double, C.c_uint32, D, C.POINTER(C.c_uint32), D, D]
+    L.sr_gravity_solve_static.argtypes = [C.POINTER(sr_config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]
+    L.sr_gravity_solve_static.restype = C.c_int
     L.sr_last_error.restype = C.c_char_p
     L.sr_last_error.argtypes = [P]
     for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_step", "sr_read_dt",
