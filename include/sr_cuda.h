@@ -190,6 +190,23 @@ sr_status sr_read_cost(sr_ctx* ctx, sr_cost* out);
 sr_status sr_heat_first_solve(sr_ctx* ctx, double dt, uint32_t precond, double* ms, uint32_t* rounds,
                               double* rel_residual, double* x);
 
+/* ---- Batches: many independent worlds of uneven sizes advanced together (the reference runs one world per Step,
+ * crates/sr-engine/src/step/mod.rs:367-718; a batch is N such Steps whose kernels overlap on one GPU). Each world keeps
+ * its own context and stream; sr_batch_step hands the worlds to a pool of host threads balanced by cell count, so the
+ * worlds' kernels (and their implicit solves' host decisions) interleave on the device. */
+typedef struct sr_batch sr_batch;
+/* `count` configurations; `threads` host threads (0: one per world, at most 16). */
+sr_status sr_batch_create(const sr_config* cfgs, uint32_t count, uint32_t threads, sr_batch** out);
+void sr_batch_destroy(sr_batch* b);
+/* World `index`: its planes (as sr_upload) and, when its configuration asks for one, its opacity plane. */
+sr_status sr_batch_upload(sr_batch* b, uint32_t index, const float* planes, const float* kappa);
+/* Every world `steps` steps. `device_ms` (optional) gets the device time from the first world's start to the last
+ * world's end. */
+sr_status sr_batch_step(sr_batch* b, uint32_t steps, double* device_ms);
+sr_status sr_batch_readback(sr_batch* b, uint32_t index, float* planes);
+/* The context of world `index` (for its reports); owned by the batch. */
+sr_ctx* sr_batch_ctx(sr_batch* b, uint32_t index);
+
 /* P2's gravity solve (φ and g = -∇φ of Σ, as a context's) with no device allocation — no counterpart in the
  * reference. For callers that cannot allocate device memory: hosts that own every byte of device memory and hand their
  * plug-ins buffers (no cudaMalloc allowed), or loops that cannot afford cudaMalloc's device-wide synchronisation. The

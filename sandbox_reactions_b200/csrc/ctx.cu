@@ -477,4 +477,6 @@ sr_status sr_heat_first_solve(sr_ctx* c, double dt, uint32_t precond, double* ms
 
 const char* sr_last_error(const sr_ctx* c) { return c ? c->error.c_str() : g_create_error.c_str(); }
 
+cudaStream_t sr_ctx_stream(sr_ctx* c) { return c->stream; }
+
 }  // extern "C"

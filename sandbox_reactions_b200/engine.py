@@ -63,6 +63,15 @@ def load_library(path: str = LIB_PATH):
     L.sr_gravity_solve_static.argtypes = [C.POINTER(sr_config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]
     L.sr_gravity_solve_static.restype = C.c_int
+    L.sr_batch_create.argtypes = [C.POINTER(sr_config), C.c_uint32, C.c_uint32, C.POINTER(P)]
+    L.sr_batch_destroy.argtypes = [P]
+    L.sr_batch_upload.argtypes = [P, C.c_uint32, F, F]
+    L.sr_batch_step.argtypes = [P, C.c_uint32, D]
+    L.sr_batch_readback.argtypes = [P, C.c_uint32, F]
+    L.sr_batch_ctx.argtypes = [P, C.c_uint32]
+    L.sr_batch_ctx.restype = P
+    for name in ("sr_batch_create", "sr_batch_upload", "sr_batch_step", "sr_batch_readback"):
+        getattr(L, name).restype = C.c_int
     L.sr_last_error.restype = C.c_char_p
     L.sr_last_error.argtypes = [P]
     for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_step", "sr_read_dt",
@@ -197,3 +206,67 @@ class Step:
         self._check(self.lib.sr_heat_first_solve(self._h, dt, PRECOND[precond], C.byref(ms), C.byref(rounds),
                                                  C.byref(rel), xp))
         return ms.value, rounds.value, rel.value, x
+
+
+class Batch:
+    """Many independent worlds of uneven sizes advanced together on one GPU (sr_batch_*): each world keeps its own
+    context and stream, and a pool of host threads, balanced by cell count, steps them concurrently."""
+
+    def __init__(self, configs, threads: int = 0):
+        self.lib = load_library()
+        self.configs = list(configs)
+        arr = (sr_config * len(self.configs))(*[c.to_c() for c in self.configs])
+        h = C.c_void_p()
+        st = self.lib.sr_batch_create(arr, len(self.configs), threads, C.byref(h))
+        if st:
+            raise SrError(st, self.lib.sr_last_error(None).decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.sr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.configs)
+
+    def _check(self, st: int):
+        if st:
+            raise SrError(st, self.lib.sr_last_error(None).decode())
+
+    def upload(self, index: int, planes: np.ndarray, kappa: np.ndarray | None = None):
+        cfg = self.configs[index]
+        p = np.ascontiguousarray(planes, dtype=np.float32)
+        if p.shape != (4, cfg.height, cfg.width):
+            raise SrError(1, f"planes of shape {p.shape} for world {index}")
+        k = np.ascontiguousarray(kappa, dtype=np.float32) if kappa is not None else None
+        self._check(self.lib.sr_batch_upload(self._h, index, _fptr(p), _fptr(k) if k is not None else None))
+
+    def run(self, steps: int = 1) -> float:
+        """Every world `steps` steps; returns the device time in ms."""
+        ms = C.c_double()
+        self._check(self.lib.sr_batch_step(self._h, int(steps), C.byref(ms)))
+        return ms.value
+
+    def readback(self, index: int) -> np.ndarray:
+        cfg = self.configs[index]
+        out = np.empty((4, cfg.height, cfg.width), np.float32)
+        self._check(self.lib.sr_batch_readback(self._h, index, _fptr(out)))
+        return out
+
+    def read_heat(self, index: int) -> sr_heat_report:
+        r = sr_heat_report()
+        ctx = self.lib.sr_batch_ctx(self._h, index)
+        st = self.lib.sr_read_heat(ctx, C.byref(r))
+        if st:
+            raise SrError(st, self.lib.sr_last_error(ctx).decode())
+        return r

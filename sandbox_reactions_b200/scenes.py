@@ -162,3 +162,21 @@ def full_step(n: int = 2048, scene: int = 0, sigma0: float = 1.0, t_bg: float = 
     cfg = Config(width=n, height=n, edge="leave", limiter="mc", gamma=gamma, mu=mu, gravity=True, hydro=True,
                  heat=True, opacity_plane=True, kernel="softened", softening=1.0, t_floor=0.05)
     return cfg, _planes(sigma, u, v, p, gamma), kappa
+
+
+def batch_mix(count: int = 64, sizes=(256, 512, 1024, 2048), scene: int = 0):
+    """Config 5: `count` worlds of a seeded mix of sizes, each config 2's disk with config 3's opacity field and hot
+    spots (scenes.full_step) with its own disk mass and opacity seed. Returns the worlds' specs (n, scene, sigma0);
+    `world(spec)` builds one as (cfg, planes, kappa)."""
+    rng = np.random.default_rng(seed_of(5, 50 + scene))
+    specs = []
+    for k in range(count):
+        n = int(rng.choice(sizes))
+        mass = float(rng.uniform(0.5, 2.0))
+        specs.append((n, 100 + 1000 * scene + k, mass))
+    return specs
+
+
+def world(spec):
+    n, scene, mass = spec
+    return full_step(n, scene=scene, sigma0=mass)
