@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define SR_ABI_VERSION 1u
+#define SR_ABI_VERSION 2u
 
 typedef enum sr_status {
     SR_OK = 0,
@@ -186,9 +186,43 @@ sr_status sr_read_cost(sr_ctx* ctx, sr_cost* out);
 
 /* The first Newton pass's linear system of one implicit step on the uploaded state, solved alone to cfg.solve_tol
  * with `precond` — the reference's heat_first_system / apply_heat_precond test hooks (step/heat.rs:609-672).
- * `ms` gets the device time of the solve, `rounds` its preconditioned CG rounds; `x` (optional, W*H f64) the solution. */
+ * `ms` gets the device time of the solve, `rounds` its preconditioned CG rounds; `x` (optional, W*H f64) the solution;
+ * `fallback` (optional) 1 when the learned preconditioner stalled and MG-PCG finished the solve. */
 sr_status sr_heat_first_solve(sr_ctx* ctx, double dt, uint32_t precond, double* ms, uint32_t* rounds,
-                              double* rel_residual, double* x);
+                              double* rel_residual, double* x, uint32_t* fallback);
+
+/* ---- The learned preconditioner — no counterpart in the reference (its preconditioners are MG and Jacobi,
+ * step/heat.rs:137-141). A 4-level convolutional U-Net (widths 8/16/32/64, 110,153 parameters) maps the
+ * Jacobi-scaled, rms-normalised residual left by one MG V-cycle, with three operator features, to the error that
+ * cycle leaves; the preconditioner is the V-cycle plus the network's correction, applied inside flexible CG. The 3x3
+ * convolutions run as BF16 implicit GEMMs on the tcgen05 tensor cores with FP32 accumulation; the network is trained on
+ * the GPU on (residual, error) pairs that plain MG-PCG generates. When it stalls (less than a 100x residual reduction
+ * after 24 rounds, or a breakdown) plain MG-PCG finishes the solve and the report's fallback_used is set. A learner
+ * owns its weights, sample store and stream; several contexts may share one (one host thread at a time). */
+typedef struct sr_learner sr_learner;
+/* `crop` (a multiple of 8 in 16..512): the side of the training crops; `capacity`: samples held. */
+sr_status sr_learner_create(uint32_t crop, uint32_t capacity, uint64_t seed, sr_learner** out);
+void sr_learner_destroy(sr_learner* learner);
+uint32_t sr_learner_param_count(void);
+/* Parameters, per layer W[cout][3][3][cin] then b[cout], f32. */
+sr_status sr_learner_get_params(sr_learner* learner, float* theta);
+sr_status sr_learner_set_params(sr_learner* learner, const float* theta);
+/* Solves the first Newton pass's system of ctx's implicit step with dt by MG-PCG from zero and stores `crops` random
+ * crops of every round's (residual left by the V-cycle, error remaining) as samples; `samples` gets how many. */
+sr_status sr_learner_collect(sr_learner* learner, sr_ctx* ctx, double dt, uint32_t crops, uint64_t seed,
+                             uint32_t* samples);
+/* `iterations` Adam steps on random batches of `batch` samples; `loss` the mean loss of the last 10 batches. The loss
+ * of a crop is the energy δᵀÂδ left by the correction (δ = target − output, Â the crop's Jacobi-scaled operator) as a
+ * fraction of the target's energy. */
+sr_status sr_learner_train(sr_learner* learner, uint32_t iterations, uint32_t batch, double lr, uint64_t seed,
+                           double* loss);
+/* The network's loss on host features (n, 4, crop, crop) against targets (n, crop, crop), the loss gradient
+ * (param_count floats) and the output (n, crop, crop) — a hook for checking the kernels against a CPU network. */
+sr_status sr_learner_loss_grad(sr_learner* learner, const float* feats, const float* target, uint32_t n, double* loss,
+                               float* grad, float* out);
+/* Makes `learner` ctx's SR_PRECOND_LEARNED (NULL detaches it; a learned context then falls back to MG). The learner
+ * must outlive the attachment. */
+sr_status sr_attach_learner(sr_ctx* ctx, sr_learner* learner);
 
 /* ---- Batches: many independent worlds of uneven sizes advanced together (the reference runs one world per Step,
  * crates/sr-engine/src/step/mod.rs:367-718; a batch is N such Steps whose kernels overlap on one GPU). Each world keeps

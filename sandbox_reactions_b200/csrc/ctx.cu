@@ -11,6 +11,7 @@
 #include "grav.cuh"
 #include "heat.cuh"
 #include "hydro.cuh"
+#include "learned.cuh"
 
 #include <atomic>
 
@@ -23,6 +24,11 @@ void sr_set_global_error(const std::string& message) { g_create_error = message;
 void sr_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void sr_note_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
 unsigned long long sr_launches() { return g_launches.load(std::memory_order_relaxed); }
+
+struct sr_learner {
+    Learner* L = nullptr;
+    cudaStream_t stream = nullptr;  // training and weight uploads
+};
 
 struct sr_ctx {
     sr_config cfg{};
@@ -45,6 +51,7 @@ struct sr_ctx {
     float *part_rate = nullptr, *part_g = nullptr;
     long long* part_nf = nullptr;
     HeatSolver* heat = nullptr;
+    sr_learner* learner = nullptr;  // attached learned preconditioner (not owned)
     sr_heat_report heat_report{};
     bool uploaded = false;
     // timing
@@ -124,6 +131,21 @@ static sr_status guarded(sr_ctx* c, F body) {
         return e.status;
     } catch (const std::exception& e) {
         c->error = e.what();
+        return SR_E_CUDA;
+    }
+}
+
+// The same for calls without a context (the message goes where sr_last_error(NULL) reads it).
+template <class F>
+static sr_status guarded_free(F body) {
+    try {
+        body();
+        return SR_OK;
+    } catch (const SrError& e) {
+        g_create_error = e.message;
+        return e.status;
+    } catch (const std::exception& e) {
+        g_create_error = e.what();
         return SR_E_CUDA;
     }
 }
@@ -370,6 +392,8 @@ sr_status sr_step(sr_ctx* c, uint32_t steps) {
         SR_REQUIRE(c->uploaded, "sr_step: no state uploaded");
         run_steps(c, steps);
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (c->cfg.precond == SR_PRECOND_LEARNED && c->learner && learned_error(c->learner->L, c->stream))
+            throw SrError{SR_E_TIMEOUT, "a tensor-core wait of the learned preconditioner gave up"};
     });
     if (st != SR_OK) return st;
     DtRecord rec;
@@ -464,14 +488,105 @@ sr_status sr_read_cost(sr_ctx* c, sr_cost* out) {
 }
 
 sr_status sr_heat_first_solve(sr_ctx* c, double dt, uint32_t precond, double* ms, uint32_t* rounds,
-                              double* rel_residual, double* x) {
+                              double* rel_residual, double* x, uint32_t* fallback) {
     return guarded(c, [&] {
         SR_REQUIRE(c->cfg.heat, "sr_heat_first_solve: the context runs no heat pass");
         SR_REQUIRE(c->uploaded, "sr_heat_first_solve: no state uploaded");
         SR_REQUIRE(dt > 0.0, "sr_heat_first_solve: dt must be positive");
         SR_REQUIRE(precond <= SR_PRECOND_LEARNED, "unknown preconditioner");
         heat_first_solve(c->heat, planes(c), c->cfg.opacity_plane ? c->kappa : nullptr, dt, precond, c->stream, ms,
-                         rounds, rel_residual, x);
+                         rounds, rel_residual, x, fallback);
+        if (precond == SR_PRECOND_LEARNED && c->learner && learned_error(c->learner->L, c->stream))
+            throw SrError{SR_E_TIMEOUT, "a tensor-core wait of the learned preconditioner gave up"};
+    });
+}
+
+// ---- the learned preconditioner
+sr_status sr_learner_create(uint32_t crop, uint32_t capacity, uint64_t seed, sr_learner** out) {
+    return guarded_free([&] {
+        SR_REQUIRE(out, "sr_learner_create: null argument");
+        *out = nullptr;
+        sr_learner* l = new sr_learner();
+        try {
+            SR_CUDA_TRY(cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking));
+            l->L = learned_create((int)crop, (int)capacity, seed);
+        } catch (...) {
+            if (l->stream) cudaStreamDestroy(l->stream);
+            delete l;
+            throw;
+        }
+        *out = l;
+    });
+}
+
+void sr_learner_destroy(sr_learner* l) {
+    if (!l) return;
+    cudaStreamSynchronize(l->stream);
+    learned_destroy(l->L);
+    cudaStreamDestroy(l->stream);
+    delete l;
+}
+
+uint32_t sr_learner_param_count(void) { return (uint32_t)learned_param_count(); }
+
+sr_status sr_learner_get_params(sr_learner* l, float* theta) {
+    return guarded_free([&] {
+        SR_REQUIRE(l && theta, "sr_learner_get_params: null argument");
+        learned_get_params(l->L, theta);
+    });
+}
+
+sr_status sr_learner_set_params(sr_learner* l, const float* theta) {
+    return guarded_free([&] {
+        SR_REQUIRE(l && theta, "sr_learner_set_params: null argument");
+        learned_set_params(l->L, theta);
+    });
+}
+
+sr_status sr_learner_collect(sr_learner* l, sr_ctx* c, double dt, uint32_t crops, uint64_t seed, uint32_t* samples) {
+    return guarded(c, [&] {
+        SR_REQUIRE(l, "sr_learner_collect: null learner");
+        SR_REQUIRE(c->cfg.heat && c->uploaded, "sr_learner_collect: the context has no implicit step to solve");
+        SR_REQUIRE(dt > 0.0, "sr_learner_collect: dt must be positive");
+        SR_REQUIRE(crops >= 1 && crops <= 4096, "sr_learner_collect: crops must be in 1..4096");
+        const int got = heat_collect(c->heat, l->L, planes(c), c->cfg.opacity_plane ? c->kappa : nullptr, dt,
+                                     (int)crops, seed, c->stream);
+        if (samples) *samples = (uint32_t)got;
+    });
+}
+
+sr_status sr_learner_train(sr_learner* l, uint32_t iterations, uint32_t batch, double lr, uint64_t seed,
+                           double* loss) {
+    return guarded_free([&] {
+        SR_REQUIRE(l, "sr_learner_train: null learner");
+        SR_REQUIRE(batch >= 1 && batch <= 4096, "sr_learner_train: batch must be in 1..4096");
+        SR_REQUIRE(lr > 0.0 && lr < 1.0, "sr_learner_train: lr must be in (0, 1)");
+        const double v = learned_train(l->L, (int)iterations, (int)batch, lr, seed, l->stream);
+        if (learned_error(l->L, l->stream))
+            throw SrError{SR_E_TIMEOUT, "a tensor-core wait of the learned preconditioner gave up"};
+        if (loss) *loss = v;
+    });
+}
+
+sr_status sr_learner_loss_grad(sr_learner* l, const float* feats, const float* target, uint32_t n, double* loss,
+                               float* grad, float* out) {
+    return guarded_free([&] {
+        SR_REQUIRE(l && feats && target, "sr_learner_loss_grad: null argument");
+        SR_REQUIRE(n >= 1 && n <= 4096, "sr_learner_loss_grad: n must be in 1..4096");
+        const double v = learned_loss_grad(l->L, feats, target, (int)n, grad, out, l->stream);
+        if (learned_error(l->L, l->stream))
+            throw SrError{SR_E_TIMEOUT, "a tensor-core wait of the learned preconditioner gave up"};
+        if (loss) *loss = v;
+    });
+}
+
+sr_status sr_attach_learner(sr_ctx* c, sr_learner* l) {
+    return guarded(c, [&] {
+        SR_REQUIRE(c->cfg.heat, "sr_attach_learner: the context runs no heat pass");
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        heat_attach_learned(c->heat, l ? l->L : nullptr);
+        c->learner = l;
+        if (!l && c->cfg.precond == SR_PRECOND_LEARNED) c->cfg.precond = SR_PRECOND_MG;
     });
 }
 

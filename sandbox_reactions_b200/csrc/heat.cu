@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "heat.cuh"
+#include "learned.cuh"
 #include "mg.cuh"
 #include "reduce.cuh"
 
@@ -21,7 +22,7 @@ namespace {
 constexpr int RED_THREADS = 256;
 constexpr int MAX_PART = 4096;    // most CTAs of a grid-stride heat kernel
 constexpr int PART_CAP = 16384;   // partials per reduced value (the level-0 smoother's CTAs included)
-enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1,
+enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1, S_ZRO, S_MGRZ,
             S_MOVED, S_VIOL, S_RAD, S_GAIN, S_HELD, S_COUNT };
 
 // Where a kernel's grid sum goes: the partials buffer, the ticket counter and the device scalar(s).
@@ -336,6 +337,60 @@ __global__ void pcg_direction_kernel(size_t n, const double* __restrict__ scal, 
         p[i] = old_slot < 0 ? z[i] : z[i] + beta * p[i];
 }
 
+// Flexible CG (the learned preconditioner is not a fixed linear operator): the update keeps the residual it replaces,
+// <z, r_old> is formed after the preconditioner, and β = (<z, r> - <z, r_old>) / <z_old, r_old> (Polak-Ribière).
+__global__ void pcg_update_flex_kernel(size_t n, const double* __restrict__ scal, int rz_slot,
+                                       const float* __restrict__ p, const float* __restrict__ q, float* e, float* r,
+                                       float* r_old, Red R) {
+    const float alpha = (float)(scal[rz_slot] / scal[S_PQ]);
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        e[i] += alpha * p[i];
+        const float ro = r[i];
+        const float ri = ro - alpha * q[i];
+        r_old[i] = ro;
+        r[i] = ri;
+        acc += (double)ri * ri;
+    }
+    grid_sum_last1(acc, R.part, R.counter, R.out);
+}
+
+__global__ void dot_kernel(size_t n, const float* __restrict__ a, const float* __restrict__ b, Red R) {
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        acc += (double)a[i] * b[i];
+    grid_sum_last1(acc, R.part, R.counter, R.out);
+}
+
+__global__ void pcg_direction_flex_kernel(size_t n, const double* __restrict__ scal, int old_slot, int new_slot,
+                                          const float* __restrict__ z, float* p) {
+    const float beta = (float)((scal[new_slot] - scal[S_ZRO]) / scal[old_slot]);
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = z[i] + beta * p[i];
+}
+
+// The residual a V-cycle leaves, r1 = r − A z (gas cells; 0 elsewhere), and optionally ez = e + z.
+__global__ void vcycle_residual_kernel(MgLevel L, const float* __restrict__ r, const float* __restrict__ z,
+                                       const float* __restrict__ e, float* r1, float* ez) {
+    const int w = L.w, h = L.h;
+    const size_t n = (size_t)w * h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % w), y = (int)(i / w);
+        float v = 0.0f;
+        const float zi = z[i];
+        if (L.mask[i]) {
+            float az = L.c[i] * zi;
+            if (x > 0) az += L.dx[i - 1] * (zi - z[i - 1]);
+            if (x + 1 < w) az += L.dx[i] * (zi - z[i + 1]);
+            if (y > 0) az += L.dy[i - w] * (zi - z[i - w]);
+            if (y + 1 < h) az += L.dy[i] * (zi - z[i + w]);
+            v = r[i] - az;
+        }
+        r1[i] = v;
+        if (ez) ez[i] = e[i] + zi;
+    }
+}
+
 // z = r / diag (Jacobi), partials of <r, z>.
 __global__ void jacobi_kernel(MgLevel L, const float* __restrict__ r, float* z, Red R) {
     const int w = L.w, h = L.h;
@@ -566,6 +621,10 @@ struct HeatSolver {
     Multigrid mg;
     int n_gas = 0;
     RoundGraph graphs[3][2];      // one PCG round per preconditioner and <r,z> slot parity
+    Learner* learner = nullptr;   // the learned preconditioner, when attached
+    LearnedApply* lapply = nullptr;
+    float* r_old = nullptr;       // flexible CG's previous residual
+    float* ez = nullptr;          // sample collection: the iterate after each round's V-cycle
 
     Red red(int slot) { return Red{part, counter, scal + slot}; }
 
@@ -596,6 +655,11 @@ void precondition(HeatSolver* H, uint32_t precond, int rz_slot, cudaStream_t s) 
     if (precond == SR_PRECOND_JACOBI) {
         jacobi_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, H->red(rz_slot));
         sr_note_launch();
+    } else if (precond == SR_PRECOND_LEARNED) {  // z = M_mg r + N(r − A M_mg r)
+        H->mg.apply(H->r32, H->z32, H->part, H->counter, H->scal + S_MGRZ, s);
+        vcycle_residual_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, nullptr, H->q32, nullptr);
+        sr_note_launch();
+        learned_apply(H->lapply, H->mg.L[0], H->q32, H->z32, H->r32, H->z32, H->part, H->counter, H->scal + rz_slot, s);
     } else {
         H->mg.apply(H->r32, H->z32, H->part, H->counter, H->scal + rz_slot, s);
     }
@@ -604,6 +668,19 @@ void precondition(HeatSolver* H, uint32_t precond, int rz_slot, cudaStream_t s) 
 // One PCG round: q = A p, α, e += α p, r -= α q, z = M r, β, p = z + β p. `parity` picks the <r,z> slots.
 void round_launches(HeatSolver* H, uint32_t precond, int parity, cudaStream_t s) {
     const int rz_old = parity ? S_RZ1 : S_RZ0, rz_new = parity ? S_RZ0 : S_RZ1;
+    if (precond == SR_PRECOND_LEARNED) {
+        spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->red(S_PQ));
+        sr_note_launch();
+        pcg_update_flex_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
+                                                               H->r_old, H->red(S_RRI));
+        sr_note_launch();
+        precondition(H, precond, rz_new, s);
+        dot_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->z32, H->r_old, H->red(S_ZRO));
+        sr_note_launch();
+        pcg_direction_flex_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, rz_new, H->z32, H->p32);
+        sr_note_launch();
+        return;
+    }
     spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->red(S_PQ));
     sr_note_launch();
     pcg_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
@@ -642,10 +719,14 @@ struct SolveResult {
     int refinements = 0;
     double rel = 0.0;
     bool ok = true;
+    bool fallback = false;  // the learned preconditioner stalled and MG-PCG finished
 };
 
-// PCG on A32 e = r32 from e = 0 to a residual reduction `eta` or `max_it` rounds. Returns the rounds, or -1 on a
-// breakdown (a non-positive or non-finite curvature).
+constexpr int kStallRounds = 24;  // learned: rounds after which a solve that has not gained 100x falls back
+
+// PCG on A32 e = r32 from e = 0 to a residual reduction `eta` or `max_it` rounds. Returns the rounds, -1 on a
+// breakdown (a non-positive or non-finite curvature), or with the learned preconditioner -2 - rounds when it stalls
+// (a breakdown, or less than a 100x reduction after kStallRounds): plain MG-PCG then takes over.
 int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStream_t s) {
     precondition(H, precond, S_RZ0, s);
     pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, -1, S_RZ0, H->z32, H->p32);
@@ -661,8 +742,9 @@ int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStrea
         if (it == next_check || it == max_it) {
             H->read(S_PQ, 2, s);  // S_PQ, S_RRI
             const double pq = H->hscal[S_PQ], rr = H->hscal[S_RRI];
-            if (!(pq > 0.0) || !isfinite(pq) || !isfinite(rr)) return -1;
+            if (!(pq > 0.0) || !isfinite(pq) || !isfinite(rr)) return precond == SR_PRECOND_LEARNED ? -2 - it : -1;
             if (rr <= eta * eta * rr0) break;
+            if (precond == SR_PRECOND_LEARNED && it >= kStallRounds && rr > 1e-4 * rr0) return -2 - it;
             next_check = it < 4 ? it + 1 : it + 4;
         }
     }
@@ -700,6 +782,13 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         sr_note_launch();
         const double eta = std::min(0.5, std::max(H->inner_floor, 0.5 / worst));
         int it = inner_pcg(H, precond, eta, max_rounds - R.rounds, s);
+        if (it <= -2) {  // the learned preconditioner stalled: its inner solve is dropped, MG-PCG restarts from x
+            R.rounds += -2 - it;
+            R.fallback = true;
+            precond = SR_PRECOND_MG;
+            prev = INFINITY;
+            continue;
+        }
         if (it < 0) {
             R.ok = false;
             return R;
@@ -795,14 +884,84 @@ void heat_destroy(HeatSolver* H) {
     cudaFree(H->part);
     cudaFree(H->counter);
     cudaFree(H->scal);
+    cudaFree(H->r_old);
+    cudaFree(H->ez);
+    learned_apply_destroy(H->lapply);
     if (H->hscal) cudaFreeHost(H->hscal);
     H->mg.destroy();
     delete H;
 }
 
 void heat_set_precond(HeatSolver* H, uint32_t precond) {
-    if (precond == SR_PRECOND_LEARNED) throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not loaded"};
+    if (precond == SR_PRECOND_LEARNED && !H->lapply)
+        throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not attached (sr_attach_learner)"};
     H->precond = precond;
+}
+
+void heat_attach_learned(HeatSolver* H, Learner* L) {
+    for (auto& g : H->graphs[SR_PRECOND_LEARNED])
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+    learned_apply_destroy(H->lapply);
+    H->lapply = nullptr;
+    H->learner = L;
+    if (!L) {
+        if (H->precond == SR_PRECOND_LEARNED) H->precond = SR_PRECOND_MG;
+        return;
+    }
+    if (!H->r_old) SR_CUDA_TRY(cudaMalloc(&H->r_old, sizeof(float) * H->n));
+    H->lapply = learned_apply_create(L, H->w, H->h);
+}
+
+int heat_collect(HeatSolver* H, Learner* L, const float* U, const float* kappa, double dt, int crops, uint64_t seed,
+                 cudaStream_t s) {
+    setup_step(H, U, kappa, s);
+    H->read(S_HEAT0, 2, s);
+    H->n_gas = (int)H->hscal[S_NGAS];
+    build_system(H, dt, s);
+    heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->c64, H->rhs, H->kx, H->ky, H->C, H->t,
+                                                           H->x, H->r64, H->red(S_RR));
+    sr_note_launch();
+    H->read(S_RR, 1, s);
+    const double rr = H->hscal[S_RR];
+    if (!(rr > 0.0) || !isfinite(rr)) return 0;
+    const double scale = sqrt(rr / (double)std::max(1, H->n_gas));
+    scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->red(S_R32));
+    sr_note_launch();
+    if (!H->ez) SR_CUDA_TRY(cudaMalloc(&H->ez, sizeof(float) * H->n));
+    // after each V-cycle z_k = M_mg r_k: the sample (r_k − A z_k, e_k + z_k); q32 is free until the next round's SpMV
+    auto snapshot = [&] {
+        vcycle_residual_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, H->e32, H->q32, H->ez);
+        sr_note_launch();
+        learned_snapshot(L, H->mg.L[0], H->q32, H->ez, s);
+    };
+    const int before = learned_samples(L);
+    learned_begin_collect(L, H->w, H->h, crops, seed);
+    precondition(H, SR_PRECOND_MG, S_RZ0, s);
+    snapshot();
+    pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, -1, S_RZ0, H->z32, H->p32);
+    sr_note_launch();
+    H->read(S_R32, 1, s);
+    const double rr0 = H->hscal[S_R32];
+    for (int it = 0; it < 200; it++) {
+        const int rz_old = (it & 1) ? S_RZ1 : S_RZ0, rz_new = (it & 1) ? S_RZ0 : S_RZ1;
+        spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->red(S_PQ));
+        sr_note_launch();
+        pcg_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
+                                                          H->red(S_RRI));
+        sr_note_launch();
+        H->read(S_PQ, 2, s);
+        // solve on to a 1e-6 residual reduction; samples only while the remaining error is large against that
+        if (!(H->hscal[S_PQ] > 0.0) || H->hscal[S_RRI] <= 1e-12 * rr0) break;
+        precondition(H, SR_PRECOND_MG, rz_new, s);
+        if (H->hscal[S_RRI] > 1e-8 * rr0) snapshot();
+        pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, rz_new, H->z32, H->p32);
+        sr_note_launch();
+    }
+    learned_end_collect(L, H->mg.L[0], H->e32, s);
+    return learned_samples(L) - before;
 }
 
 void heat_reset(HeatSolver* H, cudaStream_t s) { SR_CUDA_TRY(cudaMemsetAsync(H->rate, 0, sizeof(double) * H->n, s)); }
@@ -855,6 +1014,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         rounds += (uint32_t)S.rounds;
         R.refinements += (uint32_t)S.refinements;
         R.rel_residual = S.rel;
+        if (S.fallback) R.fallback_used = 1;
         if (!S.ok) break;
         newton_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->cfg.newton_cell, H->gas, H->C, H->x, H->t, H->u,
                                                               H->red(S_MOVED));
@@ -904,8 +1064,9 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
 }
 
 void heat_first_solve(HeatSolver* H, const float* U, const float* kappa, double dt, uint32_t precond, cudaStream_t s,
-                      double* ms, uint32_t* rounds, double* rel_residual, double* x) {
-    if (precond == SR_PRECOND_LEARNED) throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not loaded"};
+                      double* ms, uint32_t* rounds, double* rel_residual, double* x, uint32_t* fallback) {
+    if (precond == SR_PRECOND_LEARNED && !H->lapply)
+        throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not attached (sr_attach_learner)"};
     setup_step(H, U, kappa, s);
     H->read(S_HEAT0, 2, s);
     H->n_gas = (int)H->hscal[S_NGAS];
@@ -924,6 +1085,7 @@ void heat_first_solve(HeatSolver* H, const float* U, const float* kappa, double 
     if (ms) *ms = t;
     if (rounds) *rounds = (uint32_t)S.rounds;
     if (rel_residual) *rel_residual = S.rel;
+    if (fallback) *fallback = S.fallback ? 1u : 0u;
     if (x) SR_CUDA_TRY(cudaMemcpy(x, H->x, sizeof(double) * H->n, cudaMemcpyDeviceToHost));
     SR_CUDA_TRY(cudaGetLastError());
 }

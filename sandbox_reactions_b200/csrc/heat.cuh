@@ -15,6 +15,15 @@ void heat_read_flux(HeatSolver* hs, float* fx, float* fy);
 void heat_reset(HeatSolver* hs, cudaStream_t s);
 void heat_set_precond(HeatSolver* hs, uint32_t precond);
 void heat_set_limits(HeatSolver* hs, uint32_t max_passes, uint32_t max_rounds);
-// The first Newton pass's system of a step of length dt, solved alone (timed on the device).
+// The first Newton pass's system of a step of length dt, solved alone (timed on the device); `fallback` gets 1 when
+// the learned preconditioner stalled and MG-PCG finished.
 void heat_first_solve(HeatSolver* hs, const float* U, const float* kappa, double dt, uint32_t precond, cudaStream_t s,
-                      double* ms, uint32_t* rounds, double* rel_residual, double* x);
+                      double* ms, uint32_t* rounds, double* rel_residual, double* x, uint32_t* fallback);
+
+struct Learner;
+// Makes `L` (or nothing, when null) the solver's SR_PRECOND_LEARNED: one V-cycle plus the network's correction.
+void heat_attach_learned(HeatSolver* hs, Learner* L);
+// Training samples for `L` from an MG-PCG solve of the first Newton pass's system of a step of length dt; returns how
+// many were added.
+int heat_collect(HeatSolver* hs, Learner* L, const float* U, const float* kappa, double dt, int crops, uint64_t seed,
+                 cudaStream_t s);

@@ -59,7 +59,22 @@ def load_library(path: str = LIB_PATH):
     L.sr_set_heat_limits.argtypes = [P, C.c_uint32, C.c_uint32]
     L.sr_set_timing.argtypes = [P, C.c_int32]
     L.sr_read_cost.argtypes = [P, C.POINTER(sr_cost)]
-    L.sr_heat_first_solve.argtypes = [P, C.c_double, C.c_uint32, D, C.POINTER(C.c_uint32), D, D]
+    U32P = C.POINTER(C.c_uint32)
+    L.sr_heat_first_solve.argtypes = [P, C.c_double, C.c_uint32, D, U32P, D, D, U32P]
+    L.sr_learner_create.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(P)]
+    L.sr_learner_destroy.argtypes = [P]
+    L.sr_learner_destroy.restype = None
+    L.sr_learner_param_count.argtypes = []
+    L.sr_learner_param_count.restype = C.c_uint32
+    L.sr_learner_get_params.argtypes = [P, F]
+    L.sr_learner_set_params.argtypes = [P, F]
+    L.sr_learner_collect.argtypes = [P, P, C.c_double, C.c_uint32, C.c_uint64, U32P]
+    L.sr_learner_train.argtypes = [P, C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, D]
+    L.sr_learner_loss_grad.argtypes = [P, F, F, C.c_uint32, D, F, F]
+    L.sr_attach_learner.argtypes = [P, P]
+    for name in ("sr_learner_create", "sr_learner_get_params", "sr_learner_set_params", "sr_learner_collect",
+                 "sr_learner_train", "sr_learner_loss_grad", "sr_attach_learner"):
+        getattr(L, name).restype = C.c_int
     L.sr_gravity_solve_static.argtypes = [C.POINTER(sr_config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p]
     L.sr_gravity_solve_static.restype = C.c_int
@@ -203,9 +218,16 @@ class Step:
         h, w = self.shape[1:]
         x = np.empty((h, w), np.float64) if want_x else None
         xp = x.ctypes.data_as(C.POINTER(C.c_double)) if want_x else None
+        fb = C.c_uint32()
         self._check(self.lib.sr_heat_first_solve(self._h, dt, PRECOND[precond], C.byref(ms), C.byref(rounds),
-                                                 C.byref(rel), xp))
+                                                 C.byref(rel), xp, C.byref(fb)))
+        self.last_fallback = bool(fb.value)
         return ms.value, rounds.value, rel.value, x
+
+    def attach_learner(self, learner: "Learner | None"):
+        """Makes `learner` this world's "learned" preconditioner (None detaches it)."""
+        self._check(self.lib.sr_attach_learner(self._h, learner._h if learner is not None else None))
+        self._learner = learner  # kept alive while attached
 
 
 class Batch:
@@ -270,3 +292,74 @@ class Batch:
         if st:
             raise SrError(st, self.lib.sr_last_error(ctx).decode())
         return r
+
+
+class Learner:
+    """The learned preconditioner's network, weights and training samples (sr_learner_*): no reference counterpart."""
+
+    def __init__(self, crop: int = 64, capacity: int = 4096, seed: int = 0):
+        self.lib = load_library()
+        self.crop = crop
+        h = C.c_void_p()
+        st = self.lib.sr_learner_create(crop, capacity, seed, C.byref(h))
+        if st:
+            raise SrError(st, self.lib.sr_last_error(None).decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.sr_learner_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int):
+        if st:
+            raise SrError(st, self.lib.sr_last_error(None).decode())
+
+    @property
+    def param_count(self) -> int:
+        return int(self.lib.sr_learner_param_count())
+
+    def get_params(self) -> np.ndarray:
+        theta = np.empty(self.param_count, np.float32)
+        self._check(self.lib.sr_learner_get_params(self._h, _fptr(theta)))
+        return theta
+
+    def set_params(self, theta: np.ndarray):
+        theta = np.ascontiguousarray(theta, np.float32)
+        assert theta.shape == (self.param_count,)
+        self._check(self.lib.sr_learner_set_params(self._h, _fptr(theta)))
+
+    def collect(self, step: Step, dt: float, crops: int = 16, seed: int = 0) -> int:
+        """(residual, error) samples from an MG-PCG solve of `step`'s first implicit system; returns how many."""
+        n = C.c_uint32()
+        st = self.lib.sr_learner_collect(self._h, step._h, dt, crops, seed, C.byref(n))
+        if st:
+            raise SrError(st, self.lib.sr_last_error(step._h).decode())
+        return int(n.value)
+
+    def train(self, iterations: int, batch: int = 16, lr: float = 1e-3, seed: int = 0) -> float:
+        loss = C.c_double()
+        self._check(self.lib.sr_learner_train(self._h, iterations, batch, lr, seed, C.byref(loss)))
+        return float(loss.value)
+
+    def loss_grad(self, feats: np.ndarray, target: np.ndarray):
+        """(loss, gradient, output) of the network on feats (n, 4, crop, crop) against target (n, crop, crop)."""
+        feats = np.ascontiguousarray(feats, np.float32)
+        target = np.ascontiguousarray(target, np.float32)
+        n = feats.shape[0]
+        assert feats.shape == (n, 4, self.crop, self.crop) and target.shape == (n, self.crop, self.crop)
+        grad = np.empty(self.param_count, np.float32)
+        out = np.empty((n, self.crop, self.crop), np.float32)
+        loss = C.c_double()
+        self._check(self.lib.sr_learner_loss_grad(self._h, _fptr(feats), _fptr(target), n, C.byref(loss),
+                                                  _fptr(grad), _fptr(out)))
+        return float(loss.value), grad, out
