@@ -406,6 +406,17 @@ __global__ void jacobi_kernel(MgLevel L, const float* __restrict__ r, float* z, 
     grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
+// z += v, and <r, z>.
+__global__ void add_dot_kernel(size_t n, const float* __restrict__ r, const float* __restrict__ v, float* z, Red R) {
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float zi = z[i] + v[i];
+        z[i] = zi;
+        acc += (double)r[i] * zi;
+    }
+    grid_sum_last1(acc, R.part, R.counter, R.out);
+}
+
 __global__ void correction_kernel(size_t n, const uint8_t* __restrict__ gas, const float* __restrict__ e,
                                   double scale, double* x) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -625,6 +636,7 @@ struct HeatSolver {
     LearnedApply* lapply = nullptr;
     float* r_old = nullptr;       // flexible CG's previous residual
     float* ez = nullptr;          // sample collection: the iterate after each round's V-cycle
+    float* vz = nullptr;          // the learned preconditioner's second V-cycle
 
     Red red(int slot) { return Red{part, counter, scal + slot}; }
 
@@ -655,11 +667,20 @@ void precondition(HeatSolver* H, uint32_t precond, int rz_slot, cudaStream_t s) 
     if (precond == SR_PRECOND_JACOBI) {
         jacobi_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, H->red(rz_slot));
         sr_note_launch();
-    } else if (precond == SR_PRECOND_LEARNED) {  // z = M_mg r + N(r − A M_mg r)
+    } else if (precond == SR_PRECOND_LEARNED) {
+        // V-cycle, network, V-cycle: z1 = M r; z2 = z1 + N(r − A z1); z = z2 + M (r − A z2). The network predicts the
+        // smooth error the first cycle leaves; the second cycle removes the rounding noise of its BF16 output (high
+        // frequencies, which the smoothers take out) and what remains of the smooth error.
+        const MgLevel& L0 = H->mg.L[0];
         H->mg.apply(H->r32, H->z32, H->part, H->counter, H->scal + S_MGRZ, s);
-        vcycle_residual_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->r32, H->z32, nullptr, H->q32, nullptr);
+        vcycle_residual_kernel<<<H->grid, RED_THREADS, 0, s>>>(L0, H->r32, H->z32, nullptr, H->q32, nullptr);
         sr_note_launch();
-        learned_apply(H->lapply, H->mg.L[0], H->q32, H->z32, H->r32, H->z32, H->part, H->counter, H->scal + rz_slot, s);
+        learned_apply(H->lapply, L0, H->q32, H->z32, H->r32, H->z32, H->part, H->counter, H->scal + S_MGRZ, s);
+        vcycle_residual_kernel<<<H->grid, RED_THREADS, 0, s>>>(L0, H->r32, H->z32, nullptr, H->q32, nullptr);
+        sr_note_launch();
+        H->mg.apply(H->q32, H->vz, H->part, H->counter, H->scal + S_MGRZ, s);
+        add_dot_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r32, H->vz, H->z32, H->red(rz_slot));
+        sr_note_launch();
     } else {
         H->mg.apply(H->r32, H->z32, H->part, H->counter, H->scal + rz_slot, s);
     }
@@ -886,6 +907,7 @@ void heat_destroy(HeatSolver* H) {
     cudaFree(H->scal);
     cudaFree(H->r_old);
     cudaFree(H->ez);
+    cudaFree(H->vz);
     learned_apply_destroy(H->lapply);
     if (H->hscal) cudaFreeHost(H->hscal);
     H->mg.destroy();
@@ -912,6 +934,7 @@ void heat_attach_learned(HeatSolver* H, Learner* L) {
         return;
     }
     if (!H->r_old) SR_CUDA_TRY(cudaMalloc(&H->r_old, sizeof(float) * H->n));
+    if (!H->vz) SR_CUDA_TRY(cudaMalloc(&H->vz, sizeof(float) * H->n));
     H->lapply = learned_apply_create(L, H->w, H->h);
 }
 

@@ -88,7 +88,33 @@ def test_training_on_mg_pcg_pairs_lowers_the_loss():
         assert last < 0.5 * first, (first, last)
 
 
-def test_the_untrained_network_is_exactly_the_v_cycle():
+def test_the_trained_network_gains_over_the_preconditioner_without_it():
+    """Trained on MG-PCG samples of some 256² worlds, evaluated on another world at 512²: with the network's correction
+    between its two V-cycles, flexible CG reduces the residual several times more per round than with the untrained
+    network (a zero head: the same two V-cycles and nothing between), and needs no more rounds to reach 1e-8."""
+    with Learner(crop=256, capacity=600, seed=1) as L, Learner(crop=256, capacity=1, seed=1) as U:
+        assert collect(L, 256, 1000, 32, 1) >= 100
+        L.train(1500, batch=8, lr=3e-4, seed=0)
+        cfg, P, kappa = scenes.fld(512, scene=5001)
+        res = {}
+        with Step(cfg) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            for name, lr in (("untrained", U), ("trained", L)):
+                s.attach_learner(lr)
+                s.set_heat_limits(128, 2)
+                _, r2, rel2, _ = s.heat_first_solve(cfg.dt_fixed, "learned")
+                s.set_heat_limits(128, 4096)
+                _, rounds, rel, _ = s.heat_first_solve(cfg.dt_fixed, "learned")
+                assert rel <= 1e-8 and not s.last_fallback
+                res[name] = (rel2, rounds)
+            _, res["mg"], rel, _ = s.heat_first_solve(cfg.dt_fixed, "mg")
+    assert res["trained"][0] <= 0.5 * res["untrained"][0], res
+    assert res["trained"][1] <= res["untrained"][1] < res["mg"], res
+
+
+def test_the_untrained_network_adds_nothing_to_the_v_cycles():
+    """A zero head: the learned preconditioner is two V-cycles per round, which converges no slower than one."""
     cfg, P, kappa = scenes.fld(128, scene=140)
     with Learner(crop=32, capacity=16) as L, Step(cfg) as s:
         s.upload(P)
@@ -98,7 +124,7 @@ def test_the_untrained_network_is_exactly_the_v_cycle():
         _, r_l, rel_l, x_l = s.heat_first_solve(cfg.dt_fixed, "learned", want_x=True)
         assert not s.last_fallback
     assert rel_mg <= 1e-8 and rel_l <= 1e-8
-    assert abs(r_l - r_mg) <= 4  # the same iteration up to rounding (the rounds are checked every 4)
+    assert r_l <= r_mg
     assert np.abs(x_l - x_mg).max() <= 1e-6 * np.abs(x_mg).max()
 
 
