@@ -149,23 +149,59 @@ def run_reference(args, rank, world):
     return 0
 
 
+def train_learner(train_size: int = 256, worlds: int = 32, iterations: int = 1500):
+    """The learned preconditioner trained as its tests train it: MG-PCG samples of `worlds` seeded implicit-diffusion
+    worlds of train_size² (every round's whole world), Adam on the GPU. Returns (learner, samples, seconds)."""
+    from sandbox_reactions_b200 import scenes
+    from sandbox_reactions_b200.engine import Learner, Step
+
+    t0 = time.perf_counter()
+    L = Learner(crop=train_size, capacity=20 * worlds, seed=1)
+    samples = 0
+    for k in range(worlds):
+        cfg, P, kappa = scenes.fld(train_size, scene=1000 + k)
+        with Step(cfg) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            samples += L.collect(s, cfg.dt_fixed, crops=1, seed=k)
+    loss = L.train(iterations, batch=8, lr=3e-4, seed=0)
+    return L, samples, loss, time.perf_counter() - t0
+
+
 def fld_time_to_tol(size: int):
-    """The implicit-diffusion configuration's first system solved to 1e-8 with MG-PCG and Jacobi-PCG (device ms)."""
+    """The implicit-diffusion configuration's first system (a held-out seed) solved to 1e-8 with MG-PCG, Jacobi-PCG
+    and the learned preconditioner in flexible CG (device ms of the solve; training is reported apart)."""
     from sandbox_reactions_b200 import scenes
     from sandbox_reactions_b200.engine import SrError, Step
 
     cfg, P, kappa = scenes.fld(size)
     out = {"size": size, "dt": cfg.dt_fixed}
+    learner = None
+    try:
+        learner, samples, loss, secs = train_learner()
+        out["learned_training"] = {"worlds": "32 x 256x256 (seeds 1000..1031)", "samples": samples,
+                                   "iterations": 1500, "batch": 8, "final_loss": loss, "seconds": secs}
+    except SrError as e:
+        out["learned_training"] = {"unavailable": e.message}
     with Step(cfg) as s:
         s.upload(P)
         s.upload_opacity(kappa)
+        if learner is not None:
+            s.attach_learner(learner)
         for pc in ("mg", "jacobi", "learned"):
             try:
                 s.heat_first_solve(cfg.dt_fixed, pc)  # warm-up
                 ms, rounds, rel, _ = s.heat_first_solve(cfg.dt_fixed, pc)
                 out[pc] = {"ms": ms, "rounds": rounds, "rel_residual": rel}
+                if pc == "learned":
+                    out[pc]["fallback"] = s.last_fallback
             except SrError as e:
                 out[pc] = {"unavailable": e.message}
+        s.attach_learner(None)
+    if learner is not None:
+        learner.close()
+    if "ms" in out.get("learned", {}) and "ms" in out.get("mg", {}):
+        out["learned_speedup_vs_mg"] = out["mg"]["ms"] / out["learned"]["ms"]
     return out
 
 
