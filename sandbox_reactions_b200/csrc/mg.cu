@@ -74,67 +74,86 @@ __global__ void mg_coarsen_kernel(MgLevel F, MgLevel C) {
 // half-sweeps, so the tile's result is exactly the global red-black sweeps'). PRE: from x = 0, red first, into L.x,
 // then the residual summed over each 2x2 aggregate into the coarse level's b (one more halo ring keeps the residual's
 // neighbours exact). POST: from x = L.x + ω P xc, black first, into L.x2; at level 0 `out` gets <b, x2>.
+//
+// The tile is stored split by colour (cell (lx, ly) of colour (lx + ly) & 1 at ly * HX + lx / 2 of its colour's
+// arrays), so that a half-sweep's consecutive threads update consecutive cells of one colour and read their
+// neighbours, all of the other colour, at consecutive addresses: no bank conflicts. Per cell: x, b, the inverse
+// diagonal (0 on masked and outside cells, which therefore stay 0), the couplings to +x and +y, and for PRE the mass
+// term c (the residual is taken in difference form, c x + Σ d (x − x_j), which keeps its FP32 accuracy when c is far
+// below the couplings).
+constexpr int A_X = 0, A_B = 1, A_INV = 2, A_DX = 3, A_DY = 4, A_C = 5;
+
+template <int NS, bool PRE>
+constexpr size_t smooth_smem() {
+    constexpr int H = PRE ? NS + 1 : NS;
+    constexpr int RN = (SX + 2 * H) * (SY + 2 * H);
+    return (size_t)RN * (PRE ? 6 : 5) * sizeof(float);
+}
+
 template <int NS, bool PRE>
 __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, MgLevel C, const float* __restrict__ xc,
                                                                     float omega, double* part, unsigned* counter,
                                                                     double* out) {
     constexpr int H = PRE ? NS + 1 : NS;
-    constexpr int RX = SX + 2 * H, RY = SY + 2 * H, RN = RX * RY;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float* sx = reinterpret_cast<float*>(smem_raw);
-    float* sb = sx + RN;
-    float* sdx = sb + RN;
-    float* sdy = sdx + RN;
-    float* sc = sdy + RN;
-    float* sinv = sc + RN;
-    uint8_t* sm = reinterpret_cast<uint8_t*>(sinv + RN);
+    constexpr int RX = SX + 2 * H, RY = SY + 2 * H, RN = RX * RY, HX = RX / 2, HN = HX * RY;
+    static_assert(RX % 2 == 0, "the tile's rows split evenly by colour");
+    extern __shared__ __align__(16) float smem_f[];
+    auto arr = [&](int a, int k) { return smem_f + (2 * a + k) * HN; };
     const int w = L.w, h = L.h;
-    const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * SY - H;
+    const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * SY - H;  // X0 + Y0 even: local colour = global colour
     const int tid = threadIdx.x;
-    for (int k = tid; k < RN; k += SMOOTH_THREADS) {
+    constexpr int NLOAD = (RN + SMOOTH_THREADS - 1) / SMOOTH_THREADS;
+#pragma unroll
+    for (int it = 0; it < NLOAD; it++) {
+        const int k = tid + it * SMOOTH_THREADS;
+        if (k >= RN) break;
         const int lx = k % RX, ly = k / RX;
         const int gx = X0 + lx, gy = Y0 + ly;
-        float b = 0.0f, c = 1.0f, dx = 0.0f, dy = 0.0f, x = 0.0f;
-        uint8_t m = 0;
+        float b = 0.0f, c = 1.0f, dx = 0.0f, dy = 0.0f, x = 0.0f, inv = 0.0f;
         if (gx >= 0 && gx < w && gy >= 0 && gy < h) {
             const size_t i = (size_t)gy * w + gx;
+            const bool m = L.mask[i];
             b = L.b[i];
             c = L.c[i];
             dx = L.dx[i];
             dy = L.dy[i];
-            m = L.mask[i];
-            if (!PRE) {
-                x = L.x[i];
-                if (m) x += omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
+            const float dxl = gx > 0 ? L.dx[i - 1] : 0.0f, dyu = gy > 0 ? L.dy[i - w] : 0.0f;
+            if (m) {
+                inv = 1.0f / (c + dx + dxl + dy + dyu);
+                if (!PRE) x = L.x[i] + omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
             }
         }
-        sx[k] = x;
-        sb[k] = b;
-        sdx[k] = dx;
-        sdy[k] = dy;
-        sc[k] = c;
-        sm[k] = m;
+        const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
+        arr(A_X, col)[q] = x;
+        arr(A_B, col)[q] = b;
+        arr(A_INV, col)[q] = inv;
+        arr(A_DX, col)[q] = dx;
+        arr(A_DY, col)[q] = dy;
+        if (PRE) arr(A_C, col)[q] = c;
     }
     __syncthreads();
-    for (int k = tid; k < RN; k += SMOOTH_THREADS) {
-        const int lx = k % RX, ly = k / RX;
-        sinv[k] = (lx > 0 && ly > 0 && lx < RX - 1 && ly < RY - 1)
-                      ? 1.0f / (sc[k] + sdx[k] + sdx[k - 1] + sdy[k] + sdy[k - RX])
-                      : 0.0f;
-    }
-    __syncthreads();
-    constexpr int HALF = RX / 2;
+    constexpr int NSWEEP = (HN + SMOOTH_THREADS - 1) / SMOOTH_THREADS;
+#pragma unroll 1
     for (int s = 0; s < NS; s++) {
-        const int color = PRE ? (s & 1) : 1 - (s & 1);
-        for (int k = tid; k < RY * HALF; k += SMOOTH_THREADS) {
-            const int ly = k / HALF;
-            const int lx = 2 * (k % HALF) + ((color + X0 + Y0 + ly) & 1);
-            if (lx < 1 || lx >= RX - 1 || ly < 1 || ly >= RY - 1) continue;
-            const int l = ly * RX + lx;
-            if (!sm[l]) continue;
-            sx[l] = (sb[l] + sdx[l - 1] * sx[l - 1] + sdx[l] * sx[l + 1] + sdy[l - RX] * sx[l - RX] +
-                     sdy[l] * sx[l + RX]) *
-                    sinv[l];
+        const int col = PRE ? (s & 1) : 1 - (s & 1), oth = 1 - col;
+        float* x = arr(A_X, col);
+        const float* b = arr(A_B, col);
+        const float* inv = arr(A_INV, col);
+        const float* dx = arr(A_DX, col);
+        const float* dy = arr(A_DY, col);
+        const float* xo = arr(A_X, oth);
+        const float* dxo = arr(A_DX, oth);
+        const float* dyo = arr(A_DY, oth);
+#pragma unroll
+        for (int it = 0; it < NSWEEP; it++) {
+            const int q = tid + it * SMOOTH_THREADS;
+            if (q >= HN) break;
+            const int ly = q / HX, j = q - ly * HX;
+            const int o = (col + ly) & 1, lx = 2 * j + o;
+            if (lx < 1 || lx > RX - 2 || ly < 1 || ly > RY - 2) continue;
+            const int left = q - 1 + o, right = q + o;  // the other colour's cells at lx - 1 and lx + 1
+            x[q] = (b[q] + dxo[left] * xo[left] + dx[q] * xo[right] + dyo[q - HX] * xo[q - HX] + dy[q] * xo[q + HX]) *
+                   inv[q];
         }
         __syncthreads();
     }
@@ -144,9 +163,10 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
         const int ox = k % SX, oy = k / SX;
         const int gx = X0 + H + ox, gy = Y0 + H + oy;
         if (gx < w && gy < h) {
-            const int l = (oy + H) * RX + ox + H;
-            dst[(size_t)gy * w + gx] = sx[l];
-            if (!PRE && out) acc += (double)sb[l] * (double)sx[l];
+            const int lx = ox + H, ly = oy + H, col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
+            const float xv = arr(A_X, col)[q];
+            dst[(size_t)gy * w + gx] = xv;
+            if (!PRE && out) acc += (double)arr(A_B, col)[q] * (double)xv;
         }
     }
     if (PRE) {
@@ -157,20 +177,20 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
             if (X >= C.w || Y >= C.h) continue;
             float sum = 0.0f;
 #pragma unroll
-            for (int b = 0; b < 2; b++)
+            for (int bb = 0; bb < 2; bb++)
 #pragma unroll
                 for (int a = 0; a < 2; a++) {
-                    const int gx = 2 * X + a, gy = 2 * Y + b;
-                    if (gx >= w || gy >= h) continue;
-                    const int l = (2 * cyl + b + H) * RX + 2 * cxl + a + H;
-                    if (!sm[l]) continue;
-                    const float xj = sx[l];
-                    float ax = sc[l] * xj;
-                    ax += sdx[l - 1] * (xj - sx[l - 1]);
-                    ax += sdx[l] * (xj - sx[l + 1]);
-                    ax += sdy[l - RX] * (xj - sx[l - RX]);
-                    ax += sdy[l] * (xj - sx[l + RX]);
-                    sum += sb[l] - ax;
+                    const int lx = 2 * cxl + a + H, ly = 2 * cyl + bb + H;
+                    const int col = (lx + ly) & 1, oth = 1 - col, q = ly * HX + (lx >> 1);
+                    const int o = (col + ly) & 1, left = q - 1 + o, right = q + o;
+                    const float xj = arr(A_X, col)[q];
+                    const float* xo = arr(A_X, oth);
+                    float ax = arr(A_C, col)[q] * xj;
+                    ax += arr(A_DX, oth)[left] * (xj - xo[left]);
+                    ax += arr(A_DX, col)[q] * (xj - xo[right]);
+                    ax += arr(A_DY, oth)[q - HX] * (xj - xo[q - HX]);
+                    ax += arr(A_DY, col)[q] * (xj - xo[q + HX]);
+                    sum += arr(A_B, col)[q] - ax;
                 }
             C.b[(size_t)Y * C.w + X] = C.mask[(size_t)Y * C.w + X] ? sum : 0.0f;
         }
@@ -372,13 +392,6 @@ size_t tail_smem(const Multigrid& M) {
     size_t s = 0;
     for (int l = M.tail; l < M.nlevels; l++) s += (size_t)M.L[l].w * M.L[l].h * (5 * sizeof(float) + 1);
     return (s + 15) & ~(size_t)15;
-}
-
-template <int NS, bool PRE>
-constexpr size_t smooth_smem() {
-    constexpr int H = PRE ? NS + 1 : NS;
-    constexpr int RN = (SX + 2 * H) * (SY + 2 * H);
-    return (size_t)RN * (6 * sizeof(float) + 1);
 }
 
 template <int NS, bool PRE>
