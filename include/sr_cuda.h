@@ -191,6 +191,12 @@ sr_status sr_read_cost(sr_ctx* ctx, sr_cost* out);
 sr_status sr_heat_first_solve(sr_ctx* ctx, double dt, uint32_t precond, double* ms, uint32_t* rounds,
                               double* rel_residual, double* x, uint32_t* fallback);
 
+/* A benchmark hook with no counterpart in the reference: the device time of one launch of the multigrid's level-0
+ * pre-smoother and post-smoother (the step's dominant kernels) on the last solved implicit system, each averaged over
+ * `reps` launches timed with CUDA events on the context's stream, a 256 MB buffer rewritten before each launch so the
+ * level's planes come from HBM. 0 when the world is small enough that the coarse tail covers level 0. */
+sr_status sr_time_smoother(sr_ctx* ctx, uint32_t reps, double* pre_ms, double* post_ms);
+
 /* ---- The learned preconditioner — no counterpart in the reference (its preconditioners are MG and Jacobi,
  * step/heat.rs:137-141). A 4-level convolutional U-Net (widths 8/16/32/64, 110,153 parameters) maps the
  * Jacobi-scaled, rms-normalised residual left by one MG V-cycle, with three operator features, to the error that

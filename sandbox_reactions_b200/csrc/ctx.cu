@@ -501,6 +501,14 @@ sr_status sr_heat_first_solve(sr_ctx* c, double dt, uint32_t precond, double* ms
     });
 }
 
+sr_status sr_time_smoother(sr_ctx* c, uint32_t reps, double* pre_ms, double* post_ms) {
+    return guarded(c, [&] {
+        SR_REQUIRE(c->cfg.heat, "sr_time_smoother: the context runs no heat pass");
+        SR_REQUIRE(pre_ms && post_ms && reps >= 1, "sr_time_smoother: bad arguments");
+        heat_time_smoother(c->heat, (int)reps, c->stream, pre_ms, post_ms);
+    });
+}
+
 // ---- the learned preconditioner
 sr_status sr_learner_create(uint32_t crop, uint32_t capacity, uint64_t seed, sr_learner** out) {
     return guarded_free([&] {

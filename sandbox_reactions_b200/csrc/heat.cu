@@ -232,50 +232,62 @@ __global__ void heat_system_kernel(HeatConst K, double dt, const uint8_t* __rest
 }
 
 // r = b - A x in FP64, A x = c x + Σ_gas D (x_i - x_j), with partials of <r, r>, <b, b> and the reference's two
-// measures (heat.rs:413-447): rᵀD⁻¹r and the heat measure Σ (C/Δt)(r (dT/du) / D_ii)².
+// measures (heat.rs:413-447): rᵀD⁻¹r and the heat measure Σ (C/Δt)(r (dT/du) / D_ii)². Each thread takes ILP cells a
+// grid stride apart and issues all of their loads before the arithmetic (the loads do not depend on the gas flags:
+// the flags select afterwards), so a thread keeps several DRAM requests in flight.
+constexpr int ILP = 4;
+
 __global__ void heat_residual64_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
                                        const double* __restrict__ c64, const double* __restrict__ rhs,
                                        const double* __restrict__ kx, const double* __restrict__ ky,
                                        const double* __restrict__ C, const double* __restrict__ t,
-                                       const double* __restrict__ x, double* r, Red R) {
+                                       const double* __restrict__ x, double* __restrict__ r, Red R) {
     const int w = K.w, h = K.h;
-    const size_t n = (size_t)w * h;
+    const size_t n = (size_t)w * h, stride = (size_t)gridDim.x * blockDim.x;
     double rr = 0.0, bb = 0.0, gg = 0.0, hh = 0.0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        if (!gas[i]) {
-            r[i] = 0.0;
-            continue;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += 2 * stride) {
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const size_t i = base + u * stride;
+            if (i >= n) break;
+            const int xx = (int)(i % w), y = (int)(i / w);
+            const bool gi = gas[i];
+            const bool gl = xx > 0 && gas[i - 1], gr = xx + 1 < w && gas[i + 1];
+            const bool gu = y > 0 && gas[i - w], gd = y + 1 < h && gas[i + w];
+            const double xi = x[i], ci = c64[i], bi = rhs[i], Ci = C[i], ti = t[i];
+            const double xl = xx > 0 ? x[i - 1] : 0.0, xr = xx + 1 < w ? x[i + 1] : 0.0;
+            const double xu = y > 0 ? x[i - w] : 0.0, xd = y + 1 < h ? x[i + w] : 0.0;
+            const double kl = kx[(size_t)y * (w + 1) + xx], kr = kx[(size_t)y * (w + 1) + xx + 1];
+            const double ku = ky[(size_t)y * w + xx], kd = ky[(size_t)(y + 1) * w + xx];
+            if (!gi) {
+                r[i] = 0.0;
+                continue;
+            }
+            double s = ci * xi, d = ci;
+            if (gl) {
+                s += kl * (xi - xl);
+                d += kl;
+            }
+            if (gr) {
+                s += kr * (xi - xr);
+                d += kr;
+            }
+            if (gu) {
+                s += ku * (xi - xu);
+                d += ku;
+            }
+            if (gd) {
+                s += kd * (xi - xd);
+                d += kd;
+            }
+            const double ri = bi - s;
+            r[i] = ri;
+            rr += ri * ri;
+            bb += bi * bi;
+            gg += ri * ri / d;
+            const double e = ri * dt_du(K, ti) / d;
+            hh += Ci / dt * e * e;
         }
-        const int xx = (int)(i % w), y = (int)(i / w);
-        const double xi = x[i];
-        double s = c64[i] * xi, d = c64[i];
-        if (xx > 0 && gas[i - 1]) {
-            const double k = kx[(size_t)y * (w + 1) + xx];
-            s += k * (xi - x[i - 1]);
-            d += k;
-        }
-        if (xx + 1 < w && gas[i + 1]) {
-            const double k = kx[(size_t)y * (w + 1) + xx + 1];
-            s += k * (xi - x[i + 1]);
-            d += k;
-        }
-        if (y > 0 && gas[i - w]) {
-            const double k = ky[(size_t)y * w + xx];
-            s += k * (xi - x[i - w]);
-            d += k;
-        }
-        if (y + 1 < h && gas[i + w]) {
-            const double k = ky[(size_t)(y + 1) * w + xx];
-            s += k * (xi - x[i + w]);
-            d += k;
-        }
-        const double ri = rhs[i] - s;
-        r[i] = ri;
-        rr += ri * ri;
-        bb += rhs[i] * rhs[i];
-        gg += ri * ri / d;
-        const double e = ri * dt_du(K, t[i]) / d;
-        hh += C[i] / dt * e * e;
     }
     const double v[4] = {rr, bb, gg, hh};
     grid_sum_last<4>(v, R.part, R.counter, R.out);
@@ -293,48 +305,101 @@ __global__ void scale_kernel(size_t n, const double* __restrict__ r64, double in
     grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
-// q = A p on level 0's FP32 operator in difference form, c p_i + Σ d (p_i - p_j); partials of <p, q>.
-__global__ void spmv_kernel(MgLevel L, const float* __restrict__ p, float* q, Red R) {
+// q = A p on level 0's FP32 operator in difference form, c p_i + Σ d (p_i - p_j); partials of <p, q>. ILP cells per
+// thread, loads first (masked cells have c = 1 and no couplings; the mask selects afterwards).
+__global__ void spmv_kernel(MgLevel L, const float* __restrict__ p, float* __restrict__ q, Red R) {
     const int w = L.w, h = L.h;
-    const size_t n = (size_t)w * h;
+    const size_t n = (size_t)w * h, stride = (size_t)gridDim.x * blockDim.x;
     double acc = 0.0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % w), y = (int)(i / w);
-        float v = 0.0f;
-        if (L.mask[i]) {
-            const float pi = p[i];
-            v = L.c[i] * pi;
-            if (x > 0) v += L.dx[i - 1] * (pi - p[i - 1]);
-            if (x + 1 < w) v += L.dx[i] * (pi - p[i + 1]);
-            if (y > 0) v += L.dy[i - w] * (pi - p[i - w]);
-            if (y + 1 < h) v += L.dy[i] * (pi - p[i + w]);
+    for (size_t base = (size_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += ILP * stride) {
+        float pv[ILP], v[ILP];
+#pragma unroll
+        for (int u = 0; u < ILP; u++) {
+            const size_t i = base + u * stride;
+            pv[u] = 0.0f;
+            v[u] = 0.0f;
+            if (i < n) {
+                const int x = (int)(i % w), y = (int)(i / w);
+                const float pi = p[i];
+                const float pl = x > 0 ? p[i - 1] : pi, pr = x + 1 < w ? p[i + 1] : pi;
+                const float pu = y > 0 ? p[i - w] : pi, pd = y + 1 < h ? p[i + w] : pi;
+                const float dl = x > 0 ? L.dx[i - 1] : 0.0f, du = y > 0 ? L.dy[i - w] : 0.0f;
+                const float dr = L.dx[i], dd = L.dy[i], c = L.c[i];
+                const bool m = L.mask[i];
+                float a = c * pi;
+                a += dl * (pi - pl);
+                a += dr * (pi - pr);
+                a += du * (pi - pu);
+                a += dd * (pi - pd);
+                pv[u] = pi;
+                v[u] = m ? a : 0.0f;
+            }
         }
-        q[i] = v;
-        acc += (double)p[i] * v;
+#pragma unroll
+        for (int u = 0; u < ILP; u++) {
+            const size_t i = base + u * stride;
+            if (i < n) {
+                q[i] = v[u];
+                acc += (double)pv[u] * v[u];
+            }
+        }
     }
     grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
 // e += α p, r -= α q (α = <r,z>/<p,q> from the device scalars), partials of <r, r>.
 __global__ void pcg_update_kernel(size_t n, const double* __restrict__ scal, int rz_slot, const float* __restrict__ p,
-                                  const float* __restrict__ q, float* e, float* r, Red R) {
+                                  const float* __restrict__ q, float* __restrict__ e, float* __restrict__ r, Red R) {
     const float alpha = (float)(scal[rz_slot] / scal[S_PQ]);
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
     double acc = 0.0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        e[i] += alpha * p[i];
-        const float ri = r[i] - alpha * q[i];
-        r[i] = ri;
-        acc += (double)ri * ri;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += ILP * stride) {
+        float pv[ILP], qv[ILP], ev[ILP], rv[ILP];
+#pragma unroll
+        for (int u = 0; u < ILP; u++) {
+            const size_t i = base + u * stride;
+            if (i < n) {
+                pv[u] = p[i];
+                qv[u] = q[i];
+                ev[u] = e[i];
+                rv[u] = r[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < ILP; u++) {
+            const size_t i = base + u * stride;
+            if (i < n) {
+                e[i] = ev[u] + alpha * pv[u];
+                const float ri = rv[u] - alpha * qv[u];
+                r[i] = ri;
+                acc += (double)ri * ri;
+            }
+        }
     }
     grid_sum_last1(acc, R.part, R.counter, R.out);
 }
 
 // p = z + β p (β = <r,z>_new / <r,z>_old); the first direction (old slot < 0) is p = z.
 __global__ void pcg_direction_kernel(size_t n, const double* __restrict__ scal, int old_slot, int new_slot,
-                                     const float* __restrict__ z, float* p) {
+                                     const float* __restrict__ z, float* __restrict__ p) {
     const float beta = old_slot < 0 ? 0.0f : (float)(scal[new_slot] / scal[old_slot]);
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        p[i] = old_slot < 0 ? z[i] : z[i] + beta * p[i];
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t base = (size_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += ILP * stride) {
+        float zv[ILP], pv[ILP];
+#pragma unroll
+        for (int u = 0; u < ILP; u++) {
+            const size_t i = base + u * stride;
+            if (i < n) {
+                zv[u] = z[i];
+                pv[u] = old_slot < 0 ? 0.0f : p[i];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < ILP; u++) {
+            const size_t i = base + u * stride;
+            if (i < n) p[i] = old_slot < 0 ? zv[u] : zv[u] + beta * pv[u];
+        }
+    }
 }
 
 // Flexible CG (the learned preconditioner is not a fixed linear operator): the update keeps the residual it replaces,
@@ -637,6 +702,7 @@ struct HeatSolver {
     float* r_old = nullptr;       // flexible CG's previous residual
     float* ez = nullptr;          // sample collection: the iterate after each round's V-cycle
     float* vz = nullptr;          // the learned preconditioner's second V-cycle
+    void* flush = nullptr;        // timing hook: a buffer larger than L2
 
     Red red(int slot) { return Red{part, counter, scal + slot}; }
 
@@ -908,6 +974,7 @@ void heat_destroy(HeatSolver* H) {
     cudaFree(H->r_old);
     cudaFree(H->ez);
     cudaFree(H->vz);
+    cudaFree(H->flush);
     learned_apply_destroy(H->lapply);
     if (H->hscal) cudaFreeHost(H->hscal);
     H->mg.destroy();
@@ -1111,4 +1178,10 @@ void heat_first_solve(HeatSolver* H, const float* U, const float* kappa, double 
     if (fallback) *fallback = S.fallback ? 1u : 0u;
     if (x) SR_CUDA_TRY(cudaMemcpy(x, H->x, sizeof(double) * H->n, cudaMemcpyDeviceToHost));
     SR_CUDA_TRY(cudaGetLastError());
+}
+
+void heat_time_smoother(HeatSolver* H, int reps, cudaStream_t s, double* pre_ms, double* post_ms) {
+    constexpr size_t kFlush = (size_t)256 << 20;  // twice the L2
+    if (!H->flush) SR_CUDA_TRY(cudaMalloc(&H->flush, kFlush));
+    H->mg.time_level0(reps, H->flush, kFlush, s, pre_ms, post_ms);
 }

@@ -27,3 +27,5 @@ void heat_attach_learned(HeatSolver* hs, Learner* L);
 // many were added.
 int heat_collect(HeatSolver* hs, Learner* L, const float* U, const float* kappa, double dt, int crops, uint64_t seed,
                  cudaStream_t s);
+// The level-0 smoothers of the last solved system, timed alone (mg.cuh time_level0): a benchmark hook.
+void heat_time_smoother(HeatSolver* hs, int reps, cudaStream_t s, double* pre_ms, double* post_ms);

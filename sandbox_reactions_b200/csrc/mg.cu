@@ -118,9 +118,11 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
             dx = L.dx[i];
             dy = L.dy[i];
             const float dxl = gx > 0 ? L.dx[i - 1] : 0.0f, dyu = gy > 0 ? L.dy[i - w] : 0.0f;
+            float xp = 0.0f;
+            if (!PRE) xp = L.x[i] + omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];  // loads before the mask test
             if (m) {
                 inv = 1.0f / (c + dx + dxl + dy + dyu);
-                if (!PRE) x = L.x[i] + omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
+                x = xp;
             }
         }
         const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
@@ -529,4 +531,32 @@ void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter,
     for (int l = tail - 1; l >= 0; l--)
         smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, l == 0 ? part : nullptr, l == 0 ? counter : nullptr,
                l == 0 ? rz_out : nullptr, s);
+}
+
+void Multigrid::time_level0(int reps, void* flush, size_t flush_bytes, cudaStream_t s, double* pre_ms,
+                            double* post_ms) {
+    *pre_ms = *post_ms = 0.0;
+    if (tail == 0 || !L[0].b || !L[0].x2 || reps < 1) return;
+    cudaEvent_t a, b;
+    SR_CUDA_TRY(cudaEventCreate(&a));
+    SR_CUDA_TRY(cudaEventCreate(&b));
+    for (int which = 0; which < 2; which++) {
+        double total = 0.0;
+        for (int k = 0; k < reps; k++) {
+            SR_CUDA_TRY(cudaMemsetAsync(flush, k & 0xff, flush_bytes, s));
+            SR_CUDA_TRY(cudaEventRecord(a, s));
+            if (which == 0)
+                smooth(pre, true, L[0], L[1], nullptr, omega, nullptr, nullptr, nullptr, s);
+            else
+                smooth(post, false, L[0], L[1], L[1].x2, omega, nullptr, nullptr, nullptr, s);
+            SR_CUDA_TRY(cudaEventRecord(b, s));
+            SR_CUDA_TRY(cudaEventSynchronize(b));
+            float t = 0.0f;
+            SR_CUDA_TRY(cudaEventElapsedTime(&t, a, b));
+            total += t;
+        }
+        (which ? *post_ms : *pre_ms) = total / reps;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
 }

@@ -72,6 +72,8 @@ def load_library(path: str = LIB_PATH):
     L.sr_learner_train.argtypes = [P, C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, D]
     L.sr_learner_loss_grad.argtypes = [P, F, F, C.c_uint32, D, F, F]
     L.sr_attach_learner.argtypes = [P, P]
+    L.sr_time_smoother.argtypes = [P, C.c_uint32, D, D]
+    L.sr_time_smoother.restype = C.c_int
     for name in ("sr_learner_create", "sr_learner_get_params", "sr_learner_set_params", "sr_learner_collect",
                  "sr_learner_train", "sr_learner_loss_grad", "sr_attach_learner"):
         getattr(L, name).restype = C.c_int
@@ -223,6 +225,12 @@ class Step:
                                                  C.byref(rel), xp, C.byref(fb)))
         self.last_fallback = bool(fb.value)
         return ms.value, rounds.value, rel.value, x
+
+    def time_smoother(self, reps: int = 10):
+        """(pre ms, post ms): one launch of the level-0 smoothers on the last solved system, L2 flushed before each."""
+        pre, post = C.c_double(), C.c_double()
+        self._check(self.lib.sr_time_smoother(self._h, reps, C.byref(pre), C.byref(post)))
+        return pre.value, post.value
 
     def attach_learner(self, learner: "Learner | None"):
         """Makes `learner` this world's "learned" preconditioner (None detaches it)."""
