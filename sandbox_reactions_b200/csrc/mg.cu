@@ -78,9 +78,11 @@ __global__ void mg_coarsen_kernel(MgLevel F, MgLevel C) {
 // The tile is stored split by colour (cell (lx, ly) of colour (lx + ly) & 1 at ly * HX + lx / 2 of its colour's
 // arrays), so that a half-sweep's consecutive threads update consecutive cells of one colour and read their
 // neighbours, all of the other colour, at consecutive addresses: no bank conflicts. Per cell: x, b, the inverse
-// diagonal (0 on masked and outside cells, which therefore stay 0), the couplings to +x and +y, and for PRE the mass
-// term c (the residual is taken in difference form, c x + Σ d (x − x_j), which keeps its FP32 accuracy when c is far
-// below the couplings).
+// diagonal, the couplings to +x and +y, and for PRE the mass term c (the residual is taken in difference form,
+// c x + Σ d (x − x_j), which keeps its FP32 accuracy when c is far below the couplings). The mask is not read: a
+// masked cell has b = 0, c = 1 and no couplings (nor do its neighbours towards it), so its update is 0 and it
+// influences nobody; the cells outside the world get the same values. Each thread's cells of a half-sweep are the
+// same in every half-sweep of a colour: their indices and validity are computed once.
 constexpr int A_X = 0, A_B = 1, A_INV = 2, A_DX = 3, A_DY = 4, A_C = 5;
 
 template <int NS, bool PRE>
@@ -112,18 +114,13 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
         float b = 0.0f, c = 1.0f, dx = 0.0f, dy = 0.0f, x = 0.0f, inv = 0.0f;
         if (gx >= 0 && gx < w && gy >= 0 && gy < h) {
             const size_t i = (size_t)gy * w + gx;
-            const bool m = L.mask[i];
             b = L.b[i];
             c = L.c[i];
             dx = L.dx[i];
             dy = L.dy[i];
             const float dxl = gx > 0 ? L.dx[i - 1] : 0.0f, dyu = gy > 0 ? L.dy[i - w] : 0.0f;
-            float xp = 0.0f;
-            if (!PRE) xp = L.x[i] + omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];  // loads before the mask test
-            if (m) {
-                inv = 1.0f / (c + dx + dxl + dy + dyu);
-                x = xp;
-            }
+            if (!PRE) x = L.x[i] + omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
+            inv = 1.0f / (c + dx + dxl + dy + dyu);
         }
         const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
         arr(A_X, col)[q] = x;
@@ -135,6 +132,20 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
     }
     __syncthreads();
     constexpr int NSWEEP = (HN + SMOOTH_THREADS - 1) / SMOOTH_THREADS;
+    int qinfo[NSWEEP];  // per cell slot: q | o of colour 0 << 28 | updatable in colour 0 << 29 | in colour 1 << 30
+#pragma unroll
+    for (int it = 0; it < NSWEEP; it++) {
+        const int q = tid + it * SMOOTH_THREADS;
+        int info = -1;
+        if (q < HN) {
+            const int ly = q / HX, j = q - ly * HX;
+            const bool yok = ly >= 1 && ly <= RY - 2;
+            const int o0 = ly & 1, lx0 = 2 * j + o0, lx1 = 2 * j + 1 - o0;
+            const int ok0 = yok && lx0 >= 1 && lx0 <= RX - 2, ok1 = yok && lx1 >= 1 && lx1 <= RX - 2;
+            info = q | (o0 << 28) | (ok0 << 29) | (ok1 << 30);
+        }
+        qinfo[it] = info;
+    }
 #pragma unroll 1
     for (int s = 0; s < NS; s++) {
         const int col = PRE ? (s & 1) : 1 - (s & 1), oth = 1 - col;
@@ -148,11 +159,9 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
         const float* dyo = arr(A_DY, oth);
 #pragma unroll
         for (int it = 0; it < NSWEEP; it++) {
-            const int q = tid + it * SMOOTH_THREADS;
-            if (q >= HN) break;
-            const int ly = q / HX, j = q - ly * HX;
-            const int o = (col + ly) & 1, lx = 2 * j + o;
-            if (lx < 1 || lx > RX - 2 || ly < 1 || ly > RY - 2) continue;
+            const int info = qinfo[it];
+            if (info < 0 || !((info >> (29 + col)) & 1)) continue;
+            const int q = info & 0x0FFFFFFF, o = ((info >> 28) & 1) ^ col;
             const int left = q - 1 + o, right = q + o;  // the other colour's cells at lx - 1 and lx + 1
             x[q] = (b[q] + dxo[left] * xo[left] + dx[q] * xo[right] + dyo[q - HX] * xo[q - HX] + dy[q] * xo[q + HX]) *
                    inv[q];
@@ -253,7 +262,7 @@ struct TailLevel {
 
 // Threads of the tail run as 32 x 32: thread (tx, ty) takes rows ty, ty + 32, ... and, of a sweep's colour, the
 // columns 2 tx + parity, 2 (tx + 32) + parity, ... (no index divisions).
-__device__ void tail_sweep(const TailLevel& T, int color) {
+__device__ __forceinline__ void tail_sweep(const TailLevel T, int color) {
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int y = ty; y < T.h; y += 32) {
         const int par = (y + color) & 1;
@@ -273,7 +282,7 @@ __device__ void tail_sweep(const TailLevel& T, int color) {
     __syncthreads();
 }
 
-__device__ void tail_restrict(const TailLevel& F, const TailLevel& C) {
+__device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel C) {
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int Y = ty; Y < C.h; Y += 32)
         for (int X = tx; X < C.w; X += 32) {
@@ -301,25 +310,32 @@ __device__ void tail_restrict(const TailLevel& F, const TailLevel& C) {
 
 __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    TailLevel T[kMgMaxLevels];
+    __shared__ TailLevel T[kMgMaxLevels];  // in shared memory: indexed by a run-time level, so never in registers
     // carve shared memory: five float arrays per level, then the masks
     size_t off = 0;
     for (int l = A.t; l < A.nl; l++) {
         const int n = A.L[l].w * A.L[l].h;
         float* base = reinterpret_cast<float*>(smem_raw + off);
-        T[l].w = A.L[l].w;
-        T[l].h = A.L[l].h;
-        T[l].c = base;
-        T[l].dx = base + n;
-        T[l].dy = base + 2 * n;
-        T[l].b = base + 3 * n;
-        T[l].x = base + 4 * n;
+        if (threadIdx.x == 0) {
+            T[l].w = A.L[l].w;
+            T[l].h = A.L[l].h;
+            T[l].c = base;
+            T[l].dx = base + n;
+            T[l].dy = base + 2 * n;
+            T[l].b = base + 3 * n;
+            T[l].x = base + 4 * n;
+        }
         off += sizeof(float) * 5 * (size_t)n;
     }
+    const int nc = A.L[A.nl - 1].w * A.L[A.nl - 1].h;
+    float* sinv = reinterpret_cast<float*>(smem_raw + off);  // the coarsest level's inverse, nc x nc
+    off += sizeof(float) * (size_t)nc * nc;
     for (int l = A.t; l < A.nl; l++) {
-        T[l].m = reinterpret_cast<uint8_t*>(smem_raw + off);
+        if (threadIdx.x == 0) T[l].m = reinterpret_cast<uint8_t*>(smem_raw + off);
         off += (size_t)A.L[l].w * A.L[l].h;
     }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nc * nc; k += TAIL_THREADS) sinv[k] = A.coarse_inv[k];
     for (int l = A.t; l < A.nl; l++) {
         const int n = T[l].w * T[l].h;
         for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
@@ -341,12 +357,15 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
     }
     {
         // the coarsest level exactly: x = A⁻¹ b with the inverse built once per Newton pass (mg_coarse_inverse_kernel)
+        // one warp per row, the lanes splitting the row and summing by shuffles
         const TailLevel& Cs = T[A.nl - 1];
-        const int n = Cs.w * Cs.h;
-        for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int i = warp; i < nc; i += TAIL_THREADS / 32) {
             float s = 0.0f;
-            for (int k = 0; k < n; k++) s += A.coarse_inv[i * n + k] * Cs.b[k];
-            Cs.x[i] = Cs.m[i] ? s : 0.0f;
+            for (int k = lane; k < nc; k += 32) s += sinv[i * nc + k] * Cs.b[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+            if (lane == 0) Cs.x[i] = Cs.m[i] ? s : 0.0f;
         }
         __syncthreads();
     }
@@ -393,6 +412,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
 size_t tail_smem(const Multigrid& M) {
     size_t s = 0;
     for (int l = M.tail; l < M.nlevels; l++) s += (size_t)M.L[l].w * M.L[l].h * (5 * sizeof(float) + 1);
+    const size_t nc = (size_t)M.L[M.nlevels - 1].w * M.L[M.nlevels - 1].h;
+    s += sizeof(float) * nc * nc;
     return (s + 15) & ~(size_t)15;
 }
 
