@@ -22,7 +22,7 @@ namespace {
 constexpr int RED_THREADS = 256;
 constexpr int MAX_PART = 4096;    // most CTAs of a grid-stride heat kernel
 constexpr int PART_CAP = 16384;   // partials per reduced value (the level-0 smoother's CTAs included)
-enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1, S_ZRO, S_MGRZ,
+enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1, S_ZRO, S_MGRZ, S_BETA,
             S_MOVED, S_VIOL, S_RAD, S_GAIN, S_HELD, S_COUNT };
 
 // Where a kernel's grid sum goes: the partials buffer, the ticket counter and the device scalar(s).
@@ -402,6 +402,79 @@ __global__ void pcg_direction_kernel(size_t n, const double* __restrict__ scal, 
     }
 }
 
+// The fused round head of (non-flexible) PCG: the search direction p_new = z + β p (β = <r,z>_cur / <r,z>_prev, or
+// p_new = z while the S_BETA flag is 0: the first round) and q = A p_new in difference form, with partials of
+// <p_new, q>; the last CTA sets the flag. Four consecutive cells of a row per thread with 16-byte loads (W is a
+// multiple of 8); the neighbours' p_new are formed from their z and old p, so p_new goes to its own buffer.
+__global__ void spmv_dir_kernel(MgLevel L, const double* __restrict__ scal, int cur, int prev,
+                                const float* __restrict__ z, const float* __restrict__ p, float* __restrict__ pnew,
+                                float* __restrict__ q, Red R, double* beta_flag) {
+    const bool first = scal[S_BETA] == 0.0;  // p = z: the old direction is not read (it may hold anything)
+    const float beta = first ? 0.0f : (float)(scal[cur] / scal[prev]);
+    const int w = L.w, h = L.h;
+    const size_t n4 = (size_t)w * h / 4, stride = (size_t)gridDim.x * blockDim.x;
+    double acc = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += stride) {
+        const size_t i = 4 * t;
+        const int x = (int)(i % w), y = (int)(i / w);
+        auto pn4 = [&](size_t j) {
+            const float4 zz = *reinterpret_cast<const float4*>(z + j);
+            if (first) return zz;
+            const float4 pp = *reinterpret_cast<const float4*>(p + j);
+            return make_float4(zz.x + beta * pp.x, zz.y + beta * pp.y, zz.z + beta * pp.z, zz.w + beta * pp.w);
+        };
+        auto pn1 = [&](size_t j) { return first ? z[j] : z[j] + beta * p[j]; };
+        const float4 pc = pn4(i);
+        const float4 pu = y > 0 ? pn4(i - w) : pc, pd = y + 1 < h ? pn4(i + w) : pc;
+        const float pl = x > 0 ? pn1(i - 1) : pc.x;
+        const float pr = x + 4 < w ? pn1(i + 4) : pc.w;
+        const float4 c = *reinterpret_cast<const float4*>(L.c + i);
+        const float4 dx = *reinterpret_cast<const float4*>(L.dx + i), dy = *reinterpret_cast<const float4*>(L.dy + i);
+        const float dxl = x > 0 ? L.dx[i - 1] : 0.0f;
+        const float4 dyu = y > 0 ? *reinterpret_cast<const float4*>(L.dy + i - w) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const uchar4 m = *reinterpret_cast<const uchar4*>(L.mask + i);
+        const float P[6] = {pl, pc.x, pc.y, pc.z, pc.w, pr};
+        const float U[4] = {pu.x, pu.y, pu.z, pu.w}, D[4] = {pd.x, pd.y, pd.z, pd.w};
+        const float CC[4] = {c.x, c.y, c.z, c.w}, DXs[5] = {dxl, dx.x, dx.y, dx.z, dx.w};
+        const float DYu[4] = {dyu.x, dyu.y, dyu.z, dyu.w}, DYd[4] = {dy.x, dy.y, dy.z, dy.w};
+        const unsigned char M[4] = {m.x, m.y, m.z, m.w};
+        float out[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float pi = P[k + 1];
+            float a = CC[k] * pi;
+            a += DXs[k] * (pi - P[k]);
+            a += DXs[k + 1] * (pi - P[k + 2]);
+            a += DYu[k] * (pi - U[k]);
+            a += DYd[k] * (pi - D[k]);
+            out[k] = M[k] ? a : 0.0f;
+            acc += (double)pi * out[k];
+        }
+        *reinterpret_cast<float4*>(pnew + i) = pc;
+        *reinterpret_cast<float4*>(q + i) = make_float4(out[0], out[1], out[2], out[3]);
+    }
+    // the last CTA raises the flag: every CTA read it before taking its ticket
+    if (grid_sum_last1(acc, R.part, R.counter, R.out) && threadIdx.x == 0 && beta_flag) *beta_flag = 1.0;
+}
+
+// e += α p, r -= α q with 16-byte accesses (four cells per thread); partials of <r, r>.
+__global__ void pcg_update4_kernel(size_t n, const double* __restrict__ scal, int rz_slot, const float* __restrict__ p,
+                                   const float* __restrict__ q, float* __restrict__ e, float* __restrict__ r, Red R) {
+    const float alpha = (float)(scal[rz_slot] / scal[S_PQ]);
+    const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
+    double acc = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += stride) {
+        const float4 pv = reinterpret_cast<const float4*>(p)[t], qv = reinterpret_cast<const float4*>(q)[t];
+        float4 ev = reinterpret_cast<float4*>(e)[t], rv = reinterpret_cast<float4*>(r)[t];
+        ev.x += alpha * pv.x; ev.y += alpha * pv.y; ev.z += alpha * pv.z; ev.w += alpha * pv.w;
+        rv.x -= alpha * qv.x; rv.y -= alpha * qv.y; rv.z -= alpha * qv.z; rv.w -= alpha * qv.w;
+        reinterpret_cast<float4*>(e)[t] = ev;
+        reinterpret_cast<float4*>(r)[t] = rv;
+        acc += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+    }
+    grid_sum_last1(acc, R.part, R.counter, R.out);
+}
+
 // Flexible CG (the learned preconditioner is not a fixed linear operator): the update keeps the residual it replaces,
 // <z, r_old> is formed after the preconditioner, and β = (<z, r> - <z, r_old>) / <z_old, r_old> (Polak-Ribière).
 __global__ void pcg_update_flex_kernel(size_t n, const double* __restrict__ scal, int rz_slot,
@@ -689,6 +762,7 @@ struct HeatSolver {
     double* rate = nullptr;      // each cell's P5 rate (T - T⁰)/Δt in the last step, for the next first iterate
     float *kap = nullptr, *sig = nullptr;
     float *r32 = nullptr, *e32 = nullptr, *p32 = nullptr, *q32 = nullptr, *z32 = nullptr;
+    float* p2 = nullptr;  // the fused rounds' second direction buffer (rounds alternate p32 -> p2 -> p32)
     float *fx = nullptr, *fy = nullptr;
     double* part = nullptr;      // grid-sum partials: 4 x PART_CAP
     unsigned* counter = nullptr;  // grid-sum ticket
@@ -768,14 +842,17 @@ void round_launches(HeatSolver* H, uint32_t precond, int parity, cudaStream_t s)
         sr_note_launch();
         return;
     }
-    spmv_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->p32, H->q32, H->red(S_PQ));
+    // rz_old holds this round's <r, z>, rz_new the previous round's (then the next round's, after the preconditioner);
+    // the direction is read from one buffer and written to the other (neighbours read the old one)
+    float* pin = parity ? H->p2 : H->p32;
+    float* pout = parity ? H->p32 : H->p2;
+    spmv_dir_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->scal, rz_old, rz_new, H->z32, pin, pout, H->q32,
+                                                    H->red(S_PQ), H->scal + S_BETA);
     sr_note_launch();
-    pcg_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, H->p32, H->q32, H->e32, H->r32,
-                                                      H->red(S_RRI));
+    pcg_update4_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, pout, H->q32, H->e32, H->r32,
+                                                       H->red(S_RRI));
     sr_note_launch();
     precondition(H, precond, rz_new, s);
-    pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, rz_new, H->z32, H->p32);
-    sr_note_launch();
 }
 
 // A round as one CUDA graph launch (captured once per preconditioner and parity; every pointer it reads is fixed).
@@ -816,8 +893,12 @@ constexpr int kStallRounds = 24;  // learned: rounds after which a solve that ha
 // (a breakdown, or less than a 100x reduction after kStallRounds): plain MG-PCG then takes over.
 int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStream_t s) {
     precondition(H, precond, S_RZ0, s);
-    pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, -1, S_RZ0, H->z32, H->p32);
-    sr_note_launch();
+    if (precond == SR_PRECOND_LEARNED) {  // flexible CG forms its direction at the end of a round
+        pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, -1, S_RZ0, H->z32, H->p32);
+        sr_note_launch();
+    } else {  // the first round's fused direction is p = z
+        SR_CUDA_TRY(cudaMemsetAsync(H->scal + S_BETA, 0, sizeof(double), s));
+    }
     H->read(S_R32, 1, s);  // <r, r> of the scaled residual (written by scale_kernel)
     const double rr0 = H->hscal[S_R32];
     if (!(rr0 > 0.0)) return 0;
@@ -933,7 +1014,7 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         SR_CUDA_TRY(cudaMemset(H->rate, 0, sizeof(double) * n));
         SR_CUDA_TRY(cudaMalloc(&H->kx, sizeof(double) * nx));
         SR_CUDA_TRY(cudaMalloc(&H->ky, sizeof(double) * ny));
-        float** d32[] = {&H->kap, &H->sig, &H->r32, &H->e32, &H->p32, &H->q32, &H->z32};
+        float** d32[] = {&H->kap, &H->sig, &H->r32, &H->e32, &H->p32, &H->q32, &H->z32, &H->p2};
         for (float** p : d32) SR_CUDA_TRY(cudaMalloc(p, sizeof(float) * n));
         SR_CUDA_TRY(cudaMalloc(&H->fx, sizeof(float) * nx));
         SR_CUDA_TRY(cudaMalloc(&H->fy, sizeof(float) * ny));
@@ -966,7 +1047,7 @@ void heat_destroy(HeatSolver* H) {
     double* d64[] = {H->t0, H->C, H->t, H->u, H->ksum, H->kvac, H->c64, H->rhs, H->x, H->r64, H->lscale, H->rate,
                      H->kx, H->ky};
     for (double* p : d64) cudaFree(p);
-    float* d32[] = {H->kap, H->sig, H->r32, H->e32, H->p32, H->q32, H->z32, H->fx, H->fy};
+    float* d32[] = {H->kap, H->sig, H->r32, H->e32, H->p32, H->q32, H->z32, H->fx, H->fy, H->p2};
     for (float* p : d32) cudaFree(p);
     cudaFree(H->part);
     cudaFree(H->counter);

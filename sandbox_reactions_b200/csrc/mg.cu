@@ -6,8 +6,11 @@
 
 namespace {
 
-constexpr int SX = 64, SY = 32;  // smoother tile (outputs); even, so a tile's 2x2 aggregates stay inside it
-constexpr int SMOOTH_THREADS = 512;
+// Smoother tiles (outputs; even, so a tile's 2x2 aggregates stay inside it): 64 x 32 with 512 threads on big levels,
+// 32 x 16 with 256 threads where the big tile leaves fewer than 2 CTAs per SM (a quarter of the work per CTA: the
+// small levels are bound by one CTA's latency).
+constexpr int BIG_SX = 64, BIG_SY = 32, BIG_NT = 512;
+constexpr int SMALL_SX = 32, SMALL_SY = 16, SMALL_NT = 256;
 constexpr int TAIL_THREADS = 1024;
 
 struct TailArgs {
@@ -85,15 +88,15 @@ __global__ void mg_coarsen_kernel(MgLevel F, MgLevel C) {
 // same in every half-sweep of a colour: their indices and validity are computed once.
 constexpr int A_X = 0, A_B = 1, A_INV = 2, A_DX = 3, A_DY = 4, A_C = 5;
 
-template <int NS, bool PRE>
+template <int NS, bool PRE, int SX, int SY>
 constexpr size_t smooth_smem() {
     constexpr int H = PRE ? NS + 1 : NS;
     constexpr int RN = (SX + 2 * H) * (SY + 2 * H);
     return (size_t)RN * (PRE ? 6 : 5) * sizeof(float);
 }
 
-template <int NS, bool PRE>
-__global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, MgLevel C, const float* __restrict__ xc,
+template <int NS, bool PRE, int SX, int SY, int NT>
+__global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, const float* __restrict__ xc,
                                                                     float omega, double* part, unsigned* counter,
                                                                     double* out) {
     constexpr int H = PRE ? NS + 1 : NS;
@@ -104,10 +107,10 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
     const int w = L.w, h = L.h;
     const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * SY - H;  // X0 + Y0 even: local colour = global colour
     const int tid = threadIdx.x;
-    constexpr int NLOAD = (RN + SMOOTH_THREADS - 1) / SMOOTH_THREADS;
+    constexpr int NLOAD = (RN + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < NLOAD; it++) {
-        const int k = tid + it * SMOOTH_THREADS;
+        const int k = tid + it * NT;
         if (k >= RN) break;
         const int lx = k % RX, ly = k / RX;
         const int gx = X0 + lx, gy = Y0 + ly;
@@ -131,11 +134,11 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
         if (PRE) arr(A_C, col)[q] = c;
     }
     __syncthreads();
-    constexpr int NSWEEP = (HN + SMOOTH_THREADS - 1) / SMOOTH_THREADS;
+    constexpr int NSWEEP = (HN + NT - 1) / NT;
     int qinfo[NSWEEP];  // per cell slot: q | o of colour 0 << 28 | updatable in colour 0 << 29 | in colour 1 << 30
 #pragma unroll
     for (int it = 0; it < NSWEEP; it++) {
-        const int q = tid + it * SMOOTH_THREADS;
+        const int q = tid + it * NT;
         int info = -1;
         if (q < HN) {
             const int ly = q / HX, j = q - ly * HX;
@@ -170,7 +173,7 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
     }
     double acc = 0.0;
     float* dst = PRE ? L.x : L.x2;
-    for (int k = tid; k < SX * SY; k += SMOOTH_THREADS) {
+    for (int k = tid; k < SX * SY; k += NT) {
         const int ox = k % SX, oy = k / SX;
         const int gx = X0 + H + ox, gy = Y0 + H + oy;
         if (gx < w && gy < h) {
@@ -182,7 +185,7 @@ __global__ void __launch_bounds__(SMOOTH_THREADS) mg_smooth_kernel(MgLevel L, Mg
     }
     if (PRE) {
         // the coarse right-hand side: the residual, in difference form, summed over each aggregate of the tile
-        for (int k = tid; k < (SX / 2) * (SY / 2); k += SMOOTH_THREADS) {
+        for (int k = tid; k < (SX / 2) * (SY / 2); k += NT) {
             const int cxl = k % (SX / 2), cyl = k / (SX / 2);
             const int X = (X0 + H) / 2 + cxl, Y = (Y0 + H) / 2 + cyl;
             if (X >= C.w || Y >= C.h) continue;
@@ -417,13 +420,24 @@ size_t tail_smem(const Multigrid& M) {
     return (s + 15) & ~(size_t)15;
 }
 
+template <int NS, bool PRE, int SX, int SY, int NT>
+void launch_smooth_t(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
+                     double* out, cudaStream_t s) {
+    dim3 grid(div_up(L.w, SX), div_up(L.h, SY));
+    mg_smooth_kernel<NS, PRE, SX, SY, NT><<<grid, NT, smooth_smem<NS, PRE, SX, SY>(), s>>>(L, C, xc, omega, part,
+                                                                                          counter, out);
+    sr_note_launch();
+}
+
+bool small_tiles(const MgLevel& L) { return (size_t)div_up(L.w, BIG_SX) * div_up(L.h, BIG_SY) < 2 * 148; }
+
 template <int NS, bool PRE>
 void launch_smooth(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
                    double* out, cudaStream_t s) {
-    dim3 grid(div_up(L.w, SX), div_up(L.h, SY));
-    mg_smooth_kernel<NS, PRE><<<grid, SMOOTH_THREADS, smooth_smem<NS, PRE>(), s>>>(L, C, xc, omega, part, counter,
-                                                                                    out);
-    sr_note_launch();
+    if (small_tiles(L))
+        launch_smooth_t<NS, PRE, SMALL_SX, SMALL_SY, SMALL_NT>(L, C, xc, omega, part, counter, out, s);
+    else
+        launch_smooth_t<NS, PRE, BIG_SX, BIG_SY, BIG_NT>(L, C, xc, omega, part, counter, out, s);
 }
 
 void smooth(int nu, bool pre, const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part,
@@ -439,12 +453,18 @@ void smooth(int nu, bool pre, const MgLevel& L, const MgLevel& C, const float* x
     }
 }
 
+template <int NS, int SX, int SY, int NT>
+void set_attributes_tile() {
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true, SX, SY, NT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, true, SX, SY>()));
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false, SX, SY, NT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, false, SX, SY>()));
+}
+
 template <int NS>
 void set_attributes_ns() {
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smooth_smem<NS, true>()));
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smooth_smem<NS, false>()));
+    set_attributes_tile<NS, BIG_SX, BIG_SY, BIG_NT>();
+    set_attributes_tile<NS, SMALL_SX, SMALL_SY, SMALL_NT>();
 }
 
 int grid_for(size_t n) {

@@ -9,7 +9,7 @@
 #include <cuda_runtime.h>
 
 template <int K>
-__device__ __forceinline__ void grid_sum_last(const double (&v)[K], double* part, unsigned* counter, double* out) {
+__device__ __forceinline__ bool grid_sum_last(const double (&v)[K], double* part, unsigned* counter, double* out) {
     __shared__ double red[K][32];
     __shared__ bool last;
     const int tid = threadIdx.x + threadIdx.y * blockDim.x;
@@ -37,7 +37,7 @@ __device__ __forceinline__ void grid_sum_last(const double (&v)[K], double* part
         last = ticket == nb - 1;
     }
     __syncthreads();
-    if (!last) return;
+    if (!last) return false;
     __threadfence();
 #pragma unroll
     for (int q = 0; q < K; q++) {
@@ -57,10 +57,12 @@ __device__ __forceinline__ void grid_sum_last(const double (&v)[K], double* part
         }
         *counter = 0u;
     }
+    return true;
 }
 
 // One value.
-__device__ __forceinline__ void grid_sum_last1(double v, double* part, unsigned* counter, double* out) {
+// Returns true in the last CTA (after the totals are written).
+__device__ __forceinline__ bool grid_sum_last1(double v, double* part, unsigned* counter, double* out) {
     const double a[1] = {v};
-    grid_sum_last<1>(a, part, counter, out);
+    return grid_sum_last<1>(a, part, counter, out);
 }
