@@ -1029,7 +1029,7 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         H->mg.create(H->w, H->h, (int)cfg.mg_pre, (int)cfg.mg_post);
         H->mg.omega = cfg.mg_omega > 0.0 ? (float)cfg.mg_omega : 1.0f;
         H->inner_floor = cfg.inner_tol > 0.0 ? cfg.inner_tol : 1e-5;
-        SR_REQUIRE((size_t)div_up(H->w, 64) * div_up(H->h, 32) <= (size_t)PART_CAP, "world too large for the sums");
+        SR_REQUIRE(mg_smooth_ctas(H->w, H->h) <= (size_t)PART_CAP, "world too large for the sums");
         (void)s;
     } catch (...) {
         heat_destroy(H);

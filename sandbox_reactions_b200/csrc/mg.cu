@@ -12,6 +12,7 @@ namespace {
 constexpr int BIG_SX = 64, BIG_SY = 32, BIG_NT = 512;
 constexpr int SMALL_SX = 32, SMALL_SY = 16, SMALL_NT = 256;
 constexpr int TAIL_THREADS = 1024;
+constexpr int TAIL_ROWS = TAIL_THREADS / 32;  // the tail's threads as 32 columns x TAIL_ROWS rows
 
 struct TailArgs {
     int t, nl, pre, post;
@@ -259,27 +260,25 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
 // ---- the coarse tail: every level from t on, inside one CTA
 struct TailLevel {
     int w, h;
-    float *c, *dx, *dy, *b, *x;
+    float *c, *dx, *dy, *b, *x, *inv;  // inv: the inverse diagonal (0 on masked cells), formed once per launch
     uint8_t* m;
 };
 
-// Threads of the tail run as 32 x 32: thread (tx, ty) takes rows ty, ty + 32, ... and, of a sweep's colour, the
-// columns 2 tx + parity, 2 (tx + 32) + parity, ... (no index divisions).
+// Threads of the tail run as 32 columns x TAIL_ROWS rows: thread (tx, ty) takes rows ty, ty + TAIL_ROWS, ... and, of
+// a sweep's colour, the columns 2 tx + parity, 2 (tx + 32) + parity, ... (no index divisions).
 __device__ __forceinline__ void tail_sweep(const TailLevel T, int color) {
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int y = ty; y < T.h; y += 32) {
+    for (int y = ty; y < T.h; y += TAIL_ROWS) {
         const int par = (y + color) & 1;
         for (int x = 2 * tx + par; x < T.w; x += 64) {
+            // masked cells: b = 0, no couplings, inv = 0, so they stay 0; couplings past the edges are 0
             const int i = y * T.w + x;
-            if (!T.m[i]) continue;
-            const float dl = x > 0 ? T.dx[i - 1] : 0.0f, du = y > 0 ? T.dy[i - T.w] : 0.0f;
-            const float dr = T.dx[i], dd = T.dy[i];
             float s = T.b[i];
-            if (x > 0) s += dl * T.x[i - 1];
-            if (x + 1 < T.w) s += dr * T.x[i + 1];
-            if (y > 0) s += du * T.x[i - T.w];
-            if (y + 1 < T.h) s += dd * T.x[i + T.w];
-            T.x[i] = s / (T.c[i] + dl + dr + du + dd);
+            if (x > 0) s += T.dx[i - 1] * T.x[i - 1];
+            if (x + 1 < T.w) s += T.dx[i] * T.x[i + 1];
+            if (y > 0) s += T.dy[i - T.w] * T.x[i - T.w];
+            if (y + 1 < T.h) s += T.dy[i] * T.x[i + T.w];
+            T.x[i] = s * T.inv[i];
         }
     }
     __syncthreads();
@@ -287,7 +286,7 @@ __device__ __forceinline__ void tail_sweep(const TailLevel T, int color) {
 
 __device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel C) {
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    for (int Y = ty; Y < C.h; Y += 32)
+    for (int Y = ty; Y < C.h; Y += TAIL_ROWS)
         for (int X = tx; X < C.w; X += 32) {
             const int I = Y * C.w + X;
             float sum = 0.0f;
@@ -314,7 +313,7 @@ __device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel
 __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ TailLevel T[kMgMaxLevels];  // in shared memory: indexed by a run-time level, so never in registers
-    // carve shared memory: five float arrays per level, then the masks
+    // carve shared memory: six float arrays per level, the coarsest inverse, then the masks
     size_t off = 0;
     for (int l = A.t; l < A.nl; l++) {
         const int n = A.L[l].w * A.L[l].h;
@@ -327,8 +326,9 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
             T[l].dy = base + 2 * n;
             T[l].b = base + 3 * n;
             T[l].x = base + 4 * n;
+            T[l].inv = base + 5 * n;
         }
-        off += sizeof(float) * 5 * (size_t)n;
+        off += sizeof(float) * 6 * (size_t)n;
     }
     const int nc = A.L[A.nl - 1].w * A.L[A.nl - 1].h;
     float* sinv = reinterpret_cast<float*>(smem_raw + off);  // the coarsest level's inverse, nc x nc
@@ -348,6 +348,16 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
             T[l].m[i] = A.L[l].mask[i];
             T[l].x[i] = 0.0f;
             if (l == A.t) T[l].b[i] = A.L[l].b[i];
+        }
+    }
+    __syncthreads();
+    for (int l = A.t; l < A.nl; l++) {
+        const TailLevel Tl = T[l];
+        const int n = Tl.w * Tl.h;
+        for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
+            const int x = i % Tl.w, y = i / Tl.w;
+            const float d = Tl.c[i] + Tl.dx[i] + Tl.dy[i] + (x > 0 ? Tl.dx[i - 1] : 0.0f) + (y > 0 ? Tl.dy[i - Tl.w] : 0.0f);
+            Tl.inv[i] = Tl.m[i] ? 1.0f / d : 0.0f;
         }
     }
     __syncthreads();
@@ -379,7 +389,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
         (void)n;
         {
             const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-            for (int y = ty; y < F.h; y += 32)
+            for (int y = ty; y < F.h; y += TAIL_ROWS)
                 for (int x = tx; x < F.w; x += 32) {
                     const int i = y * F.w + x;
                     if (F.m[i]) F.x[i] += A.omega * Cs.x[(y >> 1) * Cs.w + (x >> 1)];
@@ -414,7 +424,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
 
 size_t tail_smem(const Multigrid& M) {
     size_t s = 0;
-    for (int l = M.tail; l < M.nlevels; l++) s += (size_t)M.L[l].w * M.L[l].h * (5 * sizeof(float) + 1);
+    for (int l = M.tail; l < M.nlevels; l++) s += (size_t)M.L[l].w * M.L[l].h * (6 * sizeof(float) + 1);
     const size_t nc = (size_t)M.L[M.nlevels - 1].w * M.L[M.nlevels - 1].h;
     s += sizeof(float) * nc * nc;
     return (s + 15) & ~(size_t)15;
@@ -473,6 +483,14 @@ int grid_for(size_t n) {
 }
 
 }  // namespace
+
+size_t mg_smooth_ctas(int w, int h) {
+    MgLevel L;
+    L.w = w;
+    L.h = h;
+    return small_tiles(L) ? (size_t)div_up(w, SMALL_SX) * div_up(h, SMALL_SY)
+                          : (size_t)div_up(w, BIG_SX) * div_up(h, BIG_SY);
+}
 
 void Multigrid::create(int w, int h, int pre_, int post_) {
     SR_REQUIRE(pre_ >= 1 && pre_ <= 3 && post_ >= 1 && post_ <= 3, "V-cycle sweeps must be 1..3");

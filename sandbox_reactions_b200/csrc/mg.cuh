@@ -27,6 +27,9 @@ struct MgLevel {
     float* x2 = nullptr;  // the post-smoother's result (a second buffer: neighbouring tiles read x's halo meanwhile)
 };
 
+// CTAs of one smoother launch on a w x h level (each writes one grid-sum partial at level 0).
+size_t mg_smooth_ctas(int w, int h);
+
 struct Multigrid {
     int nlevels = 0;
     int tail = 0;  // first level handled by the tail kernel
