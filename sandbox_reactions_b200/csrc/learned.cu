@@ -1,11 +1,12 @@
 // learned.cu — the learned preconditioner (see learned.cuh): network, tcgen05 convolutions, training and inference.
 //
 // Tensors are FP32 NHWC with channels padded to a multiple of 8, images stacked along N. A 3x3 convolution is an
-// implicit GEMM: M = 128 output pixels per CTA (one TMEM lane each), N = the output channels, K = 9 taps x the input
-// channels; the CTA gathers its im2col rows (applying the layer's input transform: pooling, upsampling, the skip
-// addition, or for the data gradient the ReLU mask) into shared memory as BF16 in the canonical no-swizzle K-major
-// layout, thread 0 issues tcgen05.mma (kind::f16, FP32 accumulator in TMEM) per 16 of K, commits to an mbarrier, and
-// the four warps read their 32 TMEM lanes back for the epilogue (bias, ReLU, FP32 store). Every mbarrier wait is
+// implicit GEMM: M = 128 output pixels per CTA (a 16 x 8 tile, one TMEM lane each), N = the output channels, K = 9 taps
+// x the input channels; the CTA stages its input halo once in shared memory as BF16 (applying the layer's input
+// transform: pooling, upsampling, the skip addition, or for the data gradient the ReLU mask), builds its im2col rows
+// from it in the canonical no-swizzle K-major layout, thread 0 issues tcgen05.mma (kind::f16, FP32 accumulator in
+// TMEM) per 16 of K, commits to an mbarrier, and the four warps read their 32 TMEM lanes back for the epilogue (bias,
+// ReLU, FP32 store). Every mbarrier wait is
 // bounded; a wait that gives up sets the learner's error flag and the CTA skips its store.
 #include <math.h>
 #include <string.h>
@@ -100,28 +101,36 @@ __device__ __forceinline__ void conv_input(const ConvArgs& A, int img, int yy, i
     }
 }
 
+// A CTA's output tile: 16 x 8 pixels of one image (thread t <-> pixel (t % 16, t / 16) <-> TMEM lane t), and its input
+// halo, 18 x 10 pixels, staged once in shared memory as BF16 (through the layer's input transform), from which each
+// thread builds its im2col row with 16-byte shared-memory copies (8 channels = one core-matrix row).
+constexpr int TW = 16, TH = 8, HW_ = TW + 2, HH_ = TH + 2, HP = HW_ * HH_;
+
 template <int CIN_P, int COUT_P>
 struct ConvShape {
-    static constexpr int NC = CIN_P >= 16 ? 3 : 1;           // K chunks (3 taps each, or all 9 taps)
-    static constexpr int KC = NC == 1 ? 80 : 3 * CIN_P;      // K of a chunk
-    static constexpr int KT = NC == 1 ? 80 : 9 * CIN_P;      // K of the weight image
+    static constexpr int NC = CIN_P >= 32 ? 3 : 1;           // K chunks (3 taps each, or all 9 taps)
+    static constexpr int KT = CIN_P == 8 ? 80 : 9 * CIN_P;   // K of the weight image (8 channels: 72 padded to 80)
+    static constexpr int KC = NC == 1 ? KT : 3 * CIN_P;      // K of a chunk
     static constexpr int TAPS = NC == 1 ? 9 : 3;
-    static constexpr int NBUF = NC == 1 ? 1 : 2;
+    static constexpr int NBUF = (NC == 1 || CIN_P == 64) ? 1 : 2;  // one A buffer for 64 channels: 2 CTAs per SM
     static constexpr int NM = COUT_P < 16 ? 16 : COUT_P;     // MMA N (M = 128 takes N in multiples of 16)
     static constexpr int NCOLS = NM <= 32 ? 32 : 64;         // TMEM columns (a power of two >= 32)
     static constexpr size_t SBG = (size_t)COUT_P * KT * 2;   // the weight image in global memory
     static constexpr size_t SB = (size_t)NM * KT * 2;        // in shared memory, zero rows up to NM
     static constexpr size_t SA = (size_t)128 * KC * 2;
-    static constexpr size_t SMEM = SB + NBUF * SA + 64;
+    static constexpr size_t SI = (size_t)HP * CIN_P * 2;     // the BF16 halo tile
+    static constexpr size_t SMEM = SB + NBUF * SA + SI + 64;
 };
 
 template <int CIN_P, int COUT_P>
 __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs A) {
     using S = ConvShape<CIN_P, COUT_P>;
+    constexpr int G = CIN_P / 8;  // channel groups of 16 bytes (BF16)
     extern __shared__ __align__(1024) unsigned char smem[];
     __nv_bfloat16* sB = reinterpret_cast<__nv_bfloat16*>(smem);
     unsigned char* sA = smem + S::SB;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(sA + S::NBUF * S::SA);
+    uint4* sIn = reinterpret_cast<uint4*>(sA + S::NBUF * S::SA);  // [HP][G]
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(sA + S::NBUF * S::SA + S::SI);
     uint32_t* tbase = reinterpret_cast<uint32_t*>(mbar + 2);
     const int tid = threadIdx.x, warp = tid >> 5;
     constexpr uint32_t IDESC = tc::idesc_bf16_f32(128, S::NM);
@@ -140,21 +149,45 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs A) {
         int4* d = reinterpret_cast<int4*>(sB);
         for (int i = tid; i < (int)(S::SB / 16); i += 128) d[i] = i < (int)(S::SBG / 16) ? g[i] : make_int4(0, 0, 0, 0);
     }
+    const int img = blockIdx.z, X0 = blockIdx.x * TW, Y0 = blockIdx.y * TH;
+    // the halo tile, through the input transform (zero outside the image), as BF16; a thread's items in batches of
+    // four, all of a batch's loads issued before any conversion
+    constexpr int NI = (HP * G + 127) / 128, NB = 4;
+#pragma unroll
+    for (int i0 = 0; i0 < NI; i0 += NB) {
+        float v[NB][8];
+#pragma unroll
+        for (int u = 0; u < NB; u++) {
+            const int e = tid + (i0 + u) * 128;
+            if (i0 + u < NI && e < HP * G) {
+                const int hp = e / G, g = e - hp * G;
+                const int hy = hp / HW_, hx = hp - hy * HW_;
+                conv_input<CIN_P>(A, img, Y0 + hy - 1, X0 + hx - 1, g * 8, v[u]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NB; u++) {
+            const int e = tid + (i0 + u) * 128;
+            if (i0 + u < NI && e < HP * G) {
+                uint4 packed;
+                __nv_bfloat162 h0 = __floats2bfloat162_rn(v[u][0], v[u][1]), h1 = __floats2bfloat162_rn(v[u][2], v[u][3]);
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(v[u][4], v[u][5]), h3 = __floats2bfloat162_rn(v[u][6], v[u][7]);
+                packed.x = *reinterpret_cast<uint32_t*>(&h0);
+                packed.y = *reinterpret_cast<uint32_t*>(&h1);
+                packed.z = *reinterpret_cast<uint32_t*>(&h2);
+                packed.w = *reinterpret_cast<uint32_t*>(&h3);
+                sIn[e] = packed;
+            }
+        }
+    }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = *tbase;
 
-    const long long P = (long long)A.B * A.H * A.W;
-    const long long p = (long long)blockIdx.x * 128 + tid;
-    const bool valid = p < P;
-    int img = 0, y = 0, x = 0;
-    if (valid) {
-        img = (int)(p / ((long long)A.H * A.W));
-        const int r = (int)(p - (long long)img * A.H * A.W);
-        y = r / A.W;
-        x = r - y * A.W;
-    }
+    const int px = tid % TW, py = tid / TW;
+    const int x = X0 + px, y = Y0 + py;
+    const bool valid = x < A.W && y < A.H;
     uint32_t par0 = 0u, par1 = 0u;
     bool ok = true;
     for (int c = 0; c < S::NC; c++) {
@@ -165,30 +198,18 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs A) {
             if (buf) par1 ^= 1u; else par0 ^= 1u;
         }
         unsigned char* a = sA + buf * S::SA;
+#pragma unroll
         for (int t = 0; t < S::TAPS; t++) {
             const int tap = S::NC == 1 ? t : c * 3 + t;
-            const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+            const int hp = (py + tap / 3) * HW_ + px + tap % 3;  // the halo pixel of (x + dx, y + dy)
 #pragma unroll
-            for (int g = 0; g < CIN_P / 8; g++) {
-                float v[8];
-                if (valid) {
-                    conv_input<CIN_P>(A, img, y + dy, x + dx, g * 8, v);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 8; q++) v[q] = 0.0f;
-                }
+            for (int g = 0; g < G; g++) {
                 const int k = t * CIN_P + g * 8;
-                uint4 packed;
-                __nv_bfloat162 h0 = __floats2bfloat162_rn(v[0], v[1]), h1 = __floats2bfloat162_rn(v[2], v[3]);
-                __nv_bfloat162 h2 = __floats2bfloat162_rn(v[4], v[5]), h3 = __floats2bfloat162_rn(v[6], v[7]);
-                packed.x = *reinterpret_cast<uint32_t*>(&h0);
-                packed.y = *reinterpret_cast<uint32_t*>(&h1);
-                packed.z = *reinterpret_cast<uint32_t*>(&h2);
-                packed.w = *reinterpret_cast<uint32_t*>(&h3);
-                *reinterpret_cast<uint4*>(a + ((tid / 8) * (S::KC / 8) + k / 8) * 128 + (tid % 8) * 16) = packed;
+                *reinterpret_cast<uint4*>(a + ((tid / 8) * (S::KC / 8) + k / 8) * 128 + (tid % 8) * 16) =
+                    sIn[hp * G + g];
             }
         }
-        if (S::NC == 1)  // K 72..79: zero padding to a multiple of 16
+        if (CIN_P == 8)  // K 72..79: zero padding to a multiple of 16
             *reinterpret_cast<uint4*>(a + ((tid / 8) * (S::KC / 8) + 9) * 128 + (tid % 8) * 16) = make_uint4(0, 0, 0, 0);
         tc::fence_async_smem();
         tc::fence_before_sync();
@@ -216,7 +237,7 @@ __global__ void __launch_bounds__(128) conv_tc_kernel(ConvArgs A) {
     tc::tmem_wait_ld();
     if (!ok) atomicExch(A.err, 1);
     if (valid && ok) {
-        float* o = A.out + (size_t)p * COUT_P;
+        float* o = A.out + ((((size_t)img * A.H + y) * A.W) + x) * COUT_P;
 #pragma unroll
         for (int c0 = 0; c0 < COUT_P; c0 += 4) {
             float4 q;
@@ -259,8 +280,8 @@ void conv_attributes() {
 template <int CI, int CO>
 void launch_conv_t(const ConvArgs& A, cudaStream_t s) {
     using S = ConvShape<CI, CO>;
-    const long long P = (long long)A.B * A.H * A.W;
-    conv_tc_kernel<CI, CO><<<(unsigned)((P + 127) / 128), 128, S::SMEM, s>>>(A);
+    const dim3 grid((unsigned)((A.W + TW - 1) / TW), (unsigned)((A.H + TH - 1) / TH), (unsigned)A.B);
+    conv_tc_kernel<CI, CO><<<grid, 128, S::SMEM, s>>>(A);
     sr_note_launch();
 }
 
