@@ -20,7 +20,7 @@
 namespace {
 
 constexpr int RED_THREADS = 256;
-constexpr int MAX_PART = 4096;    // most CTAs of a grid-stride heat kernel
+constexpr int MAX_PART = 1184;    // most CTAs of a grid-stride heat kernel: one wave (148 SMs x 8), few partials to sum
 constexpr int PART_CAP = 16384;   // partials per reduced value (the level-0 smoother's CTAs included)
 enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1, S_ZRO, S_MGRZ, S_BETA,
             S_MOVED, S_VIOL, S_RAD, S_GAIN, S_HELD, S_COUNT };
