@@ -913,7 +913,12 @@ int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStrea
             if (!(pq > 0.0) || !isfinite(pq) || !isfinite(rr)) return precond == SR_PRECOND_LEARNED ? -2 - it : -1;
             if (rr <= eta * eta * rr0) break;
             if (precond == SR_PRECOND_LEARNED && it >= kStallRounds && rr > 1e-4 * rr0) return -2 - it;
-            next_check = it < 4 ? it + 1 : it + 4;
+            // after the first three rounds, the next check one round before the rate seen so far (the geometric mean
+            // per round) reaches the target: each check costs a host round trip, each round past convergence a V-cycle
+            int more = 1;
+            const double ratio = pow(rr / rr0, 1.0 / it);
+            if (ratio > 0.0 && ratio < 1.0) more = (int)ceil(log(eta * eta * rr0 / rr) / log(ratio)) - 1;
+            next_check = it < 3 ? it + 1 : it + std::max(1, std::min(more, 8));
         }
     }
     return it;
