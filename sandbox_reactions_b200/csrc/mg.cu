@@ -239,14 +239,17 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
         aug[k] = v;
     }
     __syncthreads();
+    // at step p only columns p .. n + p can change: to the left the pivot row is already 0 (eliminated columns), to the
+    // right of n + p it is still 0 (the untouched identity columns)
+    const int na = n + 1;
     for (int p = 0; p < n; p++) {
         const double piv = aug[p * m + p];
         __syncthreads();
-        for (int j = threadIdx.x; j < m; j += blockDim.x) aug[p * m + j] /= piv;
+        for (int j = p + threadIdx.x; j <= n + p; j += blockDim.x) aug[p * m + j] /= piv;
         __syncthreads();
-        for (int k = threadIdx.x; k < n * m; k += blockDim.x) {
-            const int i = k / m, j = k % m;
-            if (i != p && j != p) aug[k] -= aug[i * m + p] * aug[p * m + j];
+        for (int k = threadIdx.x; k < n * na; k += blockDim.x) {
+            const int i = k / na, j = p + k % na;
+            if (i != p && j != p) aug[i * m + j] -= aug[i * m + p] * aug[p * m + j];
         }
         __syncthreads();
         // column p of the other rows, read as the elimination factor above, becomes 0
@@ -568,7 +571,7 @@ void Multigrid::coarsen(cudaStream_t s) {
     }
     const MgLevel& C = L[nlevels - 1];
     const size_t nc = (size_t)C.w * C.h;
-    mg_coarse_inverse_kernel<<<1, 512, nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
+    mg_coarse_inverse_kernel<<<1, 1024, nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
     sr_note_launch();
 }
 
