@@ -1,4 +1,7 @@
 // mg.cu — the multigrid V-cycle (FP32) of the implicit FLD solve; see mg.cuh for the scheme.
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "mg.cuh"
@@ -446,23 +449,24 @@ bool small_tiles(const MgLevel& L) { return (size_t)div_up(L.w, BIG_SX) * div_up
 
 template <int NS, bool PRE>
 void launch_smooth(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
-                   double* out, cudaStream_t s) {
-    if (small_tiles(L))
+                   double* out, int tile, cudaStream_t s) {
+    if (tile < 0 ? small_tiles(L) : tile == 1)
         launch_smooth_t<NS, PRE, SMALL_SX, SMALL_SY, SMALL_NT>(L, C, xc, omega, part, counter, out, s);
     else
         launch_smooth_t<NS, PRE, BIG_SX, BIG_SY, BIG_NT>(L, C, xc, omega, part, counter, out, s);
 }
 
+// `tile`: 0 the big tile, 1 the small one, -1 by the CTA-count rule (small_tiles).
 void smooth(int nu, bool pre, const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part,
-            unsigned* counter, double* out, cudaStream_t s) {
+            unsigned* counter, double* out, cudaStream_t s, int tile = -1) {
     if (pre) {
-        if (nu == 1) launch_smooth<2, true>(L, C, xc, omega, part, counter, out, s);
-        else if (nu == 2) launch_smooth<4, true>(L, C, xc, omega, part, counter, out, s);
-        else launch_smooth<6, true>(L, C, xc, omega, part, counter, out, s);
+        if (nu == 1) launch_smooth<2, true>(L, C, xc, omega, part, counter, out, tile, s);
+        else if (nu == 2) launch_smooth<4, true>(L, C, xc, omega, part, counter, out, tile, s);
+        else launch_smooth<6, true>(L, C, xc, omega, part, counter, out, tile, s);
     } else {
-        if (nu == 1) launch_smooth<2, false>(L, C, xc, omega, part, counter, out, s);
-        else if (nu == 2) launch_smooth<4, false>(L, C, xc, omega, part, counter, out, s);
-        else launch_smooth<6, false>(L, C, xc, omega, part, counter, out, s);
+        if (nu == 1) launch_smooth<2, false>(L, C, xc, omega, part, counter, out, tile, s);
+        else if (nu == 2) launch_smooth<4, false>(L, C, xc, omega, part, counter, out, tile, s);
+        else launch_smooth<6, false>(L, C, xc, omega, part, counter, out, tile, s);
     }
 }
 
@@ -564,6 +568,53 @@ void Multigrid::set_couplings(const double* kx, const double* ky, const uint8_t*
     sr_note_launch();
 }
 
+// The smoother tile of each level below 0 (level 0 keeps the CTA-count rule, which bounds its grid-sum partials) chosen
+// by timing: the big and the small tile, pre- and post-smoother, three launches each, on the level's current operator.
+// Choices are kept per level size for the process (a batch's worlds of one size tune once).
+void Multigrid::autotune(cudaStream_t s) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, int> chosen;
+    tuned = true;
+    for (int l = 1; l < tail; l++) {
+        const std::pair<int, int> key(L[l].w, L[l].h);
+        {
+            std::lock_guard<std::mutex> g(mu);
+            auto it = chosen.find(key);
+            if (it != chosen.end()) {
+                tile[l] = it->second;
+                continue;
+            }
+        }
+        cudaEvent_t a, b;
+        SR_CUDA_TRY(cudaEventCreate(&a));
+        SR_CUDA_TRY(cudaEventCreate(&b));
+        float best = 0.0f;
+        int pick = small_tiles(L[l]) ? 1 : 0;
+        for (int cand = 0; cand < 2; cand++) {
+            float total = 0.0f;
+            for (int rep = 0; rep < 4; rep++) {  // the first launch of each warms up
+                SR_CUDA_TRY(cudaEventRecord(a, s));
+                smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s, cand);
+                smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, nullptr, nullptr, nullptr, s, cand);
+                SR_CUDA_TRY(cudaEventRecord(b, s));
+                SR_CUDA_TRY(cudaEventSynchronize(b));
+                float t = 0.0f;
+                SR_CUDA_TRY(cudaEventElapsedTime(&t, a, b));
+                if (rep > 0) total += t;
+            }
+            if (cand == 0 || total < best) {
+                best = total;
+                pick = cand;
+            }
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        tile[l] = pick;
+        std::lock_guard<std::mutex> g(mu);
+        chosen[key] = pick;
+    }
+}
+
 void Multigrid::coarsen(cudaStream_t s) {
     for (int l = 1; l < nlevels; l++) {
         mg_coarsen_kernel<<<grid_for((size_t)L[l].w * L[l].h), 256, 0, s>>>(L[l - 1], L[l]);
@@ -573,12 +624,14 @@ void Multigrid::coarsen(cudaStream_t s) {
     const size_t nc = (size_t)C.w * C.h;
     mg_coarse_inverse_kernel<<<1, 1024, nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
     sr_note_launch();
+    if (!tuned) autotune(s);
 }
 
 void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter, double* rz_out, cudaStream_t s) {
     L[0].b = const_cast<float*>(r);
     L[0].x2 = z;
-    for (int l = 0; l < tail; l++) smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s);
+    for (int l = 0; l < tail; l++)
+        smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s, tile[l]);
     TailArgs T;
     T.coarse_inv = coarse_inv;
     T.t = tail;
@@ -592,7 +645,7 @@ void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter,
     sr_note_launch();
     for (int l = tail - 1; l >= 0; l--)
         smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, l == 0 ? part : nullptr, l == 0 ? counter : nullptr,
-               l == 0 ? rz_out : nullptr, s);
+               l == 0 ? rz_out : nullptr, s, tile[l]);
 }
 
 void Multigrid::time_level0(int reps, void* flush, size_t flush_bytes, cudaStream_t s, double* pre_ms,
@@ -608,9 +661,9 @@ void Multigrid::time_level0(int reps, void* flush, size_t flush_bytes, cudaStrea
             SR_CUDA_TRY(cudaMemsetAsync(flush, k & 0xff, flush_bytes, s));
             SR_CUDA_TRY(cudaEventRecord(a, s));
             if (which == 0)
-                smooth(pre, true, L[0], L[1], nullptr, omega, nullptr, nullptr, nullptr, s);
+                smooth(pre, true, L[0], L[1], nullptr, omega, nullptr, nullptr, nullptr, s, tile[0]);
             else
-                smooth(post, false, L[0], L[1], L[1].x2, omega, nullptr, nullptr, nullptr, s);
+                smooth(post, false, L[0], L[1], L[1].x2, omega, nullptr, nullptr, nullptr, s, tile[0]);
             SR_CUDA_TRY(cudaEventRecord(b, s));
             SR_CUDA_TRY(cudaEventSynchronize(b));
             float t = 0.0f;
