@@ -99,7 +99,7 @@ constexpr size_t smooth_smem() {
     return (size_t)RN * (PRE ? 6 : 5) * sizeof(float);
 }
 
-template <int NS, bool PRE, int SX, int SY, int NT>
+template <int NS, bool PRE, int SX, int SY, int NT, bool VEC>
 __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, const float* __restrict__ xc,
                                                                     float omega, double* part, unsigned* counter,
                                                                     double* out) {
@@ -111,6 +111,57 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
     const int w = L.w, h = L.h;
     const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * SY - H;  // X0 + Y0 even: local colour = global colour
     const int tid = threadIdx.x;
+    if constexpr (VEC) {
+        // rows in 16-byte chunks from the 4-aligned column at or left of X0 (the level's width is a multiple of 4, so a
+        // chunk lies wholly inside or wholly outside the level): 4 cells' b, c, dx, dy, the row above's dy, and for
+        // POST x and the two coarse corrections, in 6-7 loads
+        constexpr int OFF = (4 - H % 4) % 4, NCH = (OFF + RX + 3) / 4, NV = RY * NCH;
+        const int X0a = X0 - OFF;
+        constexpr int NVL = (NV + NT - 1) / NT;
+#pragma unroll
+        for (int it = 0; it < NVL; it++) {
+            const int k = tid + it * NT;
+            if (k >= NV) break;
+            const int ly = k / NCH, ch = k - ly * NCH;
+            const int gx0 = X0a + 4 * ch, gy = Y0 + ly;
+            float4 b4 = make_float4(0.f, 0.f, 0.f, 0.f), c4 = make_float4(1.f, 1.f, 1.f, 1.f), dx4 = b4, dy4 = b4,
+                   dyu4 = b4, x4 = b4;
+            float dxl = 0.0f;
+            float2 xc2 = make_float2(0.f, 0.f);
+            const bool in = gy >= 0 && gy < h && gx0 >= 0 && gx0 < w;
+            if (in) {
+                const size_t i = (size_t)gy * w + gx0;
+                b4 = *reinterpret_cast<const float4*>(L.b + i);
+                c4 = *reinterpret_cast<const float4*>(L.c + i);
+                dx4 = *reinterpret_cast<const float4*>(L.dx + i);
+                dy4 = *reinterpret_cast<const float4*>(L.dy + i);
+                if (gy > 0) dyu4 = *reinterpret_cast<const float4*>(L.dy + i - w);
+                if (gx0 > 0) dxl = L.dx[i - 1];
+                if (!PRE) {
+                    x4 = *reinterpret_cast<const float4*>(L.x + i);
+                    xc2 = *reinterpret_cast<const float2*>(xc + (size_t)(gy >> 1) * C.w + (gx0 >> 1));
+                }
+            }
+            const float bb[4] = {b4.x, b4.y, b4.z, b4.w}, cc[4] = {c4.x, c4.y, c4.z, c4.w};
+            const float dxa[5] = {dxl, dx4.x, dx4.y, dx4.z, dx4.w}, dya[4] = {dy4.x, dy4.y, dy4.z, dy4.w};
+            const float dyua[4] = {dyu4.x, dyu4.y, dyu4.z, dyu4.w}, xa[4] = {x4.x, x4.y, x4.z, x4.w};
+            const float xcv[2] = {xc2.x, xc2.y};
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const int lx = 4 * ch + e - OFF;
+                if (lx < 0 || lx >= RX) continue;
+                const float inv = in ? 1.0f / (cc[e] + dxa[e + 1] + dxa[e] + dya[e] + dyua[e]) : 0.0f;
+                const float x = (!PRE && in) ? xa[e] + omega * xcv[e >> 1] : 0.0f;
+                const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
+                arr(A_X, col)[q] = x;
+                arr(A_B, col)[q] = bb[e];
+                arr(A_INV, col)[q] = inv;
+                arr(A_DX, col)[q] = dxa[e + 1];
+                arr(A_DY, col)[q] = dya[e];
+                if (PRE) arr(A_C, col)[q] = cc[e];
+            }
+        }
+    } else {
     constexpr int NLOAD = (RN + NT - 1) / NT;
 #pragma unroll
     for (int it = 0; it < NLOAD; it++) {
@@ -136,6 +187,7 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
         arr(A_DX, col)[q] = dx;
         arr(A_DY, col)[q] = dy;
         if (PRE) arr(A_C, col)[q] = c;
+    }
     }
     __syncthreads();
     constexpr int NSWEEP = (HN + NT - 1) / NT;
@@ -440,8 +492,15 @@ template <int NS, bool PRE, int SX, int SY, int NT>
 void launch_smooth_t(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
                      double* out, cudaStream_t s) {
     dim3 grid(div_up(L.w, SX), div_up(L.h, SY));
-    mg_smooth_kernel<NS, PRE, SX, SY, NT><<<grid, NT, smooth_smem<NS, PRE, SX, SY>(), s>>>(L, C, xc, omega, part,
-                                                                                          counter, out);
+    // 16-byte rows (and 8-byte coarse pairs) stay aligned; the pre-smoother's odd halo would load 8 % more columns, and
+    // measured slower, so it keeps the per-cell loads
+    const bool vec = !PRE && L.w % 4 == 0 && C.w % 2 == 0;
+    if (vec)
+        mg_smooth_kernel<NS, PRE, SX, SY, NT, true><<<grid, NT, smooth_smem<NS, PRE, SX, SY>(), s>>>(
+            L, C, xc, omega, part, counter, out);
+    else
+        mg_smooth_kernel<NS, PRE, SX, SY, NT, false><<<grid, NT, smooth_smem<NS, PRE, SX, SY>(), s>>>(
+            L, C, xc, omega, part, counter, out);
     sr_note_launch();
 }
 
@@ -472,9 +531,13 @@ void smooth(int nu, bool pre, const MgLevel& L, const MgLevel& C, const float* x
 
 template <int NS, int SX, int SY, int NT>
 void set_attributes_tile() {
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true, SX, SY, NT>,
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true, SX, SY, NT, true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, true, SX, SY>()));
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false, SX, SY, NT>,
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false, SX, SY, NT, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, false, SX, SY>()));
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true, SX, SY, NT, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, true, SX, SY>()));
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false, SX, SY, NT, false>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, false, SX, SY>()));
 }
 
