@@ -214,7 +214,7 @@ __device__ __forceinline__ Prim P_at(const Shared& sh, int ly, int lx) {
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(NT, 2) hydro_tile_kernel(HydroArgs A) {
+__global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 CTAs per SM: 80 registers, ~15 B spilled
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Shared& sh = *reinterpret_cast<Shared*>(smem_raw);
     const HydroConst H = A.H;
