@@ -210,6 +210,32 @@ def fld_time_to_tol(size: int):
     return out
 
 
+def config_runs(peak_gbs: float):
+    """The other single-GPU configurations as side measurements (device time of the steps, library events): C1, the
+    Sod tube at 512² with minmod (hydro only, 200 steps), and C2, the disk at 1024² with its FFT gravity (100 steps);
+    each with its hydro update kernel's HBM roofline (32 B/cell without gravity, 56 B/cell with)."""
+    from sandbox_reactions_b200 import scenes
+    from sandbox_reactions_b200.engine import Step
+
+    out = {}
+    for name, (cfg, P), steps, bpc in (("C1_sod_512_minmod", scenes.sod(512), 200, 32),
+                                       ("C2_disk_hydro_grav_1024", scenes.disk(1024), 100, 56)):
+        with Step(cfg) as s:
+            s.upload(P)
+            s.run(3)
+            s.set_timing(True)
+            s.run(steps)
+            c = s.read_cost()
+        n = cfg.width * cfg.height
+        upd = c.hydro_update_ms / max(1, c.hydro_update_launches)
+        gbs = bpc * n / (upd / 1e3) / 1e9
+        out[name] = {"value": n * steps / (c.total_ms / 1e3) / 1e6, "unit": "Mcell-steps/s", "steps": steps,
+                     "ms_per_step": c.total_ms / steps,
+                     "hydro_update": {"ms_per_launch": upd, "algorithmic_bytes_per_cell": bpc, "achieved_gbs": gbs,
+                                      "frac_of_measured_hbm": gbs / peak_gbs}}
+    return out
+
+
 def run_batch(args, rank, world, local):
     """Config 5: a seeded mix of worlds split over the ranks by cell count, each rank's share advanced as one batch;
     the aggregate Mcell-steps/s beside the same worlds stepped one at a time."""
@@ -370,9 +396,11 @@ def main():
     e2e_value = world * n * n * e2e_steps / (float(t.item()) / 1e3) / 1e6
 
     fld = None
+    configs = None
     if rank == 0 and not args.no_fld and world == 1:
         step.close()
         fld = fld_time_to_tol(2048 if n >= 2048 else n)
+        configs = config_runs(measured_peaks()[0])
     step.close()
 
     if rank == 0:
@@ -422,6 +450,7 @@ def main():
             "heat_last_step": {"passes": heat.passes, "rounds": heat.rounds, "refinements": heat.refinements,
                                "converged": heat.converged, "rel_residual": heat.rel_residual},
             "fld_time_to_1e-8": fld,
+            "other_configs": configs,
         }
         print(json.dumps(line), flush=True)
     if dist:
