@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
             for (int e = 0; e < 4; e++) {
                 const int lx = 4 * ch + e - OFF;
                 if (lx < 0 || lx >= RX) continue;
-                const float inv = in ? 1.0f / (cc[e] + dxa[e + 1] + dxa[e] + dya[e] + dyua[e]) : 0.0f;
+                const float inv = in ? __fdividef(1.0f, cc[e] + dxa[e + 1] + dxa[e] + dya[e] + dyua[e]) : 0.0f;
                 const float x = (!PRE && in) ? xa[e] + omega * xcv[e >> 1] : 0.0f;
                 const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
                 arr(A_X, col)[q] = x;
@@ -171,14 +171,14 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
         const int gx = X0 + lx, gy = Y0 + ly;
         float b = 0.0f, c = 1.0f, dx = 0.0f, dy = 0.0f, x = 0.0f, inv = 0.0f;
         if (gx >= 0 && gx < w && gy >= 0 && gy < h) {
-            const size_t i = (size_t)gy * w + gx;
+            const int i = gy * w + gx;  // a level holds fewer than 2^31 cells
             b = L.b[i];
             c = L.c[i];
             dx = L.dx[i];
             dy = L.dy[i];
             const float dxl = gx > 0 ? L.dx[i - 1] : 0.0f, dyu = gy > 0 ? L.dy[i - w] : 0.0f;
             if (!PRE) x = L.x[i] + omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
-            inv = 1.0f / (c + dx + dxl + dy + dyu);
+            inv = __fdividef(1.0f, c + dx + dxl + dy + dyu);  // the smoother's diagonal: an approximate reciprocal
         }
         const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
         arr(A_X, col)[q] = x;
