@@ -316,96 +316,109 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
 }
 
 // ---- the coarse tail: every level from t on, inside one CTA
+// A level's arrays as offsets into the tail's dynamic shared memory (floats for the six arrays, bytes for the mask):
+// indexing the extern shared array itself keeps every access a shared-memory access.
+extern __shared__ __align__(16) unsigned char tail_smem_raw[];
 struct TailLevel {
     int w, h;
-    float *c, *dx, *dy, *b, *x, *inv;  // inv: the inverse diagonal (0 on masked cells), formed once per launch
-    uint8_t* m;
+    int c, dx, dy, b, x, inv;  // float offsets; inv: the inverse diagonal (0 on masked cells), formed once per launch
+    int m;                     // byte offset of the mask
 };
+__device__ __forceinline__ float* tsf() { return reinterpret_cast<float*>(tail_smem_raw); }
 
 // Threads of the tail run as 32 columns x TAIL_ROWS rows: thread (tx, ty) takes rows ty, ty + TAIL_ROWS, ... and, of
 // a sweep's colour, the columns 2 tx + parity, 2 (tx + 32) + parity, ... (no index divisions).
 __device__ __forceinline__ void tail_sweep(const TailLevel T, int color) {
+    float* f = tsf();
+    const float *b = f + T.b, *dx = f + T.dx, *dy = f + T.dy, *inv = f + T.inv;
+    float* x = f + T.x;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int y = ty; y < T.h; y += TAIL_ROWS) {
         const int par = (y + color) & 1;
-        for (int x = 2 * tx + par; x < T.w; x += 64) {
+        for (int xx = 2 * tx + par; xx < T.w; xx += 64) {
             // masked cells: b = 0, no couplings, inv = 0, so they stay 0; couplings past the edges are 0
-            const int i = y * T.w + x;
-            float s = T.b[i];
-            if (x > 0) s += T.dx[i - 1] * T.x[i - 1];
-            if (x + 1 < T.w) s += T.dx[i] * T.x[i + 1];
-            if (y > 0) s += T.dy[i - T.w] * T.x[i - T.w];
-            if (y + 1 < T.h) s += T.dy[i] * T.x[i + T.w];
-            T.x[i] = s * T.inv[i];
+            const int i = y * T.w + xx;
+            float s = b[i];
+            if (xx > 0) s += dx[i - 1] * x[i - 1];
+            if (xx + 1 < T.w) s += dx[i] * x[i + 1];
+            if (y > 0) s += dy[i - T.w] * x[i - T.w];
+            if (y + 1 < T.h) s += dy[i] * x[i + T.w];
+            x[i] = s * inv[i];
         }
     }
     __syncthreads();
 }
 
 __device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel C) {
+    float* f = tsf();
+    const float *fc = f + F.c, *fdx = f + F.dx, *fdy = f + F.dy, *fb = f + F.b, *fx = f + F.x;
+    const uint8_t* fm = tail_smem_raw + F.m;
+    const uint8_t* cm = tail_smem_raw + C.m;
+    float *cb = f + C.b, *cx = f + C.x;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     for (int Y = ty; Y < C.h; Y += TAIL_ROWS)
         for (int X = tx; X < C.w; X += 32) {
             const int I = Y * C.w + X;
             float sum = 0.0f;
-            for (int b = 0; b < 2; b++)
+            for (int bb = 0; bb < 2; bb++)
                 for (int a = 0; a < 2; a++) {
-                    const int x = 2 * X + a, y = 2 * Y + b;
+                    const int x = 2 * X + a, y = 2 * Y + bb;
                     if (x >= F.w || y >= F.h) continue;
                     const int j = y * F.w + x;
-                    if (!F.m[j]) continue;
-                    const float xj = F.x[j];
-                    float ax = F.c[j] * xj;
-                    if (x > 0) ax += F.dx[j - 1] * (xj - F.x[j - 1]);
-                    if (x + 1 < F.w) ax += F.dx[j] * (xj - F.x[j + 1]);
-                    if (y > 0) ax += F.dy[j - F.w] * (xj - F.x[j - F.w]);
-                    if (y + 1 < F.h) ax += F.dy[j] * (xj - F.x[j + F.w]);
-                    sum += F.b[j] - ax;
+                    if (!fm[j]) continue;
+                    const float xj = fx[j];
+                    float ax = fc[j] * xj;
+                    if (x > 0) ax += fdx[j - 1] * (xj - fx[j - 1]);
+                    if (x + 1 < F.w) ax += fdx[j] * (xj - fx[j + 1]);
+                    if (y > 0) ax += fdy[j - F.w] * (xj - fx[j - F.w]);
+                    if (y + 1 < F.h) ax += fdy[j] * (xj - fx[j + F.w]);
+                    sum += fb[j] - ax;
                 }
-            C.b[I] = C.m[I] ? sum : 0.0f;
-            C.x[I] = 0.0f;
+            cb[I] = cm[I] ? sum : 0.0f;
+            cx[I] = 0.0f;
         }
     __syncthreads();
 }
 
 __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ TailLevel T[kMgMaxLevels];  // in shared memory: indexed by a run-time level, so never in registers
+    float* f = tsf();
+    __shared__ TailLevel T[kMgMaxLevels];  // indexed by a run-time level
     // carve shared memory: six float arrays per level, the coarsest inverse, then the masks
-    size_t off = 0;
+    int off = 0;  // in floats
     for (int l = A.t; l < A.nl; l++) {
         const int n = A.L[l].w * A.L[l].h;
-        float* base = reinterpret_cast<float*>(smem_raw + off);
         if (threadIdx.x == 0) {
             T[l].w = A.L[l].w;
             T[l].h = A.L[l].h;
-            T[l].c = base;
-            T[l].dx = base + n;
-            T[l].dy = base + 2 * n;
-            T[l].b = base + 3 * n;
-            T[l].x = base + 4 * n;
-            T[l].inv = base + 5 * n;
+            T[l].c = off;
+            T[l].dx = off + n;
+            T[l].dy = off + 2 * n;
+            T[l].b = off + 3 * n;
+            T[l].x = off + 4 * n;
+            T[l].inv = off + 5 * n;
         }
-        off += sizeof(float) * 6 * (size_t)n;
+        off += 6 * n;
     }
     const int nc = A.L[A.nl - 1].w * A.L[A.nl - 1].h;
-    float* sinv = reinterpret_cast<float*>(smem_raw + off);  // the coarsest level's inverse, nc x nc
-    off += sizeof(float) * (size_t)nc * nc;
+    float* sinv = f + off;  // the coarsest level's inverse, nc x nc
+    off += nc * nc;
+    int moff = off * (int)sizeof(float);  // bytes
     for (int l = A.t; l < A.nl; l++) {
-        if (threadIdx.x == 0) T[l].m = reinterpret_cast<uint8_t*>(smem_raw + off);
-        off += (size_t)A.L[l].w * A.L[l].h;
+        if (threadIdx.x == 0) T[l].m = moff;
+        moff += A.L[l].w * A.L[l].h;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < nc * nc; k += TAIL_THREADS) sinv[k] = A.coarse_inv[k];
     for (int l = A.t; l < A.nl; l++) {
-        const int n = T[l].w * T[l].h;
+        const TailLevel Tl = T[l];
+        const int n = Tl.w * Tl.h;
         for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
-            T[l].c[i] = A.L[l].c[i];
-            T[l].dx[i] = A.L[l].dx[i];
-            T[l].dy[i] = A.L[l].dy[i];
-            T[l].m[i] = A.L[l].mask[i];
-            T[l].x[i] = 0.0f;
-            if (l == A.t) T[l].b[i] = A.L[l].b[i];
+            f[Tl.c + i] = A.L[l].c[i];
+            f[Tl.dx + i] = A.L[l].dx[i];
+            f[Tl.dy + i] = A.L[l].dy[i];
+            tail_smem_raw[Tl.m + i] = A.L[l].mask[i];
+            f[Tl.x + i] = 0.0f;
+            if (l == A.t) f[Tl.b + i] = A.L[l].b[i];
         }
     }
     __syncthreads();
@@ -414,43 +427,43 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
         const int n = Tl.w * Tl.h;
         for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
             const int x = i % Tl.w, y = i / Tl.w;
-            const float d = Tl.c[i] + Tl.dx[i] + Tl.dy[i] + (x > 0 ? Tl.dx[i - 1] : 0.0f) + (y > 0 ? Tl.dy[i - Tl.w] : 0.0f);
-            Tl.inv[i] = Tl.m[i] ? 1.0f / d : 0.0f;
+            const float d = f[Tl.c + i] + f[Tl.dx + i] + f[Tl.dy + i] + (x > 0 ? f[Tl.dx + i - 1] : 0.0f) +
+                            (y > 0 ? f[Tl.dy + i - Tl.w] : 0.0f);
+            f[Tl.inv + i] = tail_smem_raw[Tl.m + i] ? 1.0f / d : 0.0f;
         }
     }
     __syncthreads();
     for (int l = A.t; l < A.nl - 1; l++) {
+        const TailLevel Tl = T[l];
         for (int s = 0; s < A.pre; s++) {
-            tail_sweep(T[l], 0);
-            tail_sweep(T[l], 1);
+            tail_sweep(Tl, 0);
+            tail_sweep(Tl, 1);
         }
-        tail_restrict(T[l], T[l + 1]);
+        tail_restrict(Tl, T[l + 1]);
     }
     {
         // the coarsest level exactly: x = A⁻¹ b with the inverse built once per Newton pass (mg_coarse_inverse_kernel)
         // one warp per row, the lanes splitting the row and summing by shuffles
-        const TailLevel& Cs = T[A.nl - 1];
+        const TailLevel Cs = T[A.nl - 1];
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         for (int i = warp; i < nc; i += TAIL_THREADS / 32) {
             float s = 0.0f;
-            for (int k = lane; k < nc; k += 32) s += sinv[i * nc + k] * Cs.b[k];
+            for (int k = lane; k < nc; k += 32) s += sinv[i * nc + k] * f[Cs.b + k];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) Cs.x[i] = Cs.m[i] ? s : 0.0f;
+            if (lane == 0) f[Cs.x + i] = tail_smem_raw[Cs.m + i] ? s : 0.0f;
         }
         __syncthreads();
     }
     for (int l = A.nl - 2; l >= A.t; l--) {
-        const TailLevel& F = T[l];
-        const TailLevel& Cs = T[l + 1];
-        const int n = F.w * F.h;
-        (void)n;
+        const TailLevel F = T[l];
+        const TailLevel Cs = T[l + 1];
         {
             const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
             for (int y = ty; y < F.h; y += TAIL_ROWS)
                 for (int x = tx; x < F.w; x += 32) {
                     const int i = y * F.w + x;
-                    if (F.m[i]) F.x[i] += A.omega * Cs.x[(y >> 1) * Cs.w + (x >> 1)];
+                    if (tail_smem_raw[F.m + i]) f[F.x + i] += A.omega * f[Cs.x + (y >> 1) * Cs.w + (x >> 1)];
                 }
         }
         __syncthreads();
@@ -459,12 +472,13 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
             tail_sweep(F, 0);
         }
     }
-    const TailLevel& top = T[A.t];
+    const TailLevel top = T[A.t];
     const int n = top.w * top.h;
     double acc = 0.0;
     for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
-        A.L[A.t].x2[i] = top.x[i];
-        acc += (double)top.b[i] * (double)top.x[i];
+        const float xv = f[top.x + i];
+        A.L[A.t].x2[i] = xv;
+        acc += (double)f[top.b + i] * (double)xv;
     }
     if (A.out) {
         __shared__ double red[TAIL_THREADS / 32];
