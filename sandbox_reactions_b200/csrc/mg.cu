@@ -1,6 +1,4 @@
 // mg.cu — the multigrid V-cycle (FP32) of the implicit FLD solve; see mg.cuh for the scheme.
-#include <map>
-#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -39,9 +37,9 @@ __global__ void mg_couplings0_kernel(MgLevel L, const double* __restrict__ kx, c
     }
 }
 
-// Level l+1 from level l: Galerkin aggregation of 2x2 cells (mg.cuh). The mass term c sums over the aggregate's
-// system cells; a coarse coupling sums the two fine couplings across the aggregates' shared side.
-__global__ void mg_coarsen_kernel(MgLevel F, MgLevel C) {
+// Level 1 from level 0: Galerkin aggregation of 2x2 cells with constant weights (mg.cuh). The mass term c sums over
+// the aggregate's system cells; a coarse coupling sums the two fine couplings across the aggregates' shared side.
+__global__ void mg_aggregate_kernel(MgLevel F, MgLevel C) {
     const int wc = C.w, hc = C.h, wf = F.w, hf = F.h;
     const size_t nc = (size_t)wc * hc;
     for (size_t I = (size_t)blockIdx.x * blockDim.x + threadIdx.x; I < nc; I += (size_t)gridDim.x * blockDim.x) {
@@ -77,6 +75,112 @@ __global__ void mg_coarsen_kernel(MgLevel F, MgLevel C) {
     }
 }
 
+// Level l+1 from level l >= 1 (mg.cuh): each 2x2 aggregate's basis function is the fine weight vector t restricted to
+// the aggregate, t from two red-black Gauss-Seidel sweeps on A t = 0 from t = 1 (masked cells 0), scaled so that its
+// largest value in the aggregate is 1; the coarse operator is the Galerkin product, still 5-point:
+//   coarse coupling to +x  = sum over the two fine couplings crossing the shared side of t_j t_k d_jk,
+//   coarse c (diagonal less couplings) = sum_j t_j (A t)_j over the aggregate = (P^T A t)_I,
+// with (A t)_j = c_j t_j + sum_k d_jk (t_j - t_k) in difference form, summed in f64 from the f32 weights the
+// restriction and prolongation use. One tile of CO_S x CO_S fine cells per CTA, all four half-sweeps in shared
+// memory: the tile's halo is as deep as the half-sweeps plus the two rings whose aggregates' scale the Galerkin sums
+// read (t of the cells next to the tile's aggregates).
+constexpr int CO_S = 32, CO_H = 6, CO_R = CO_S + 2 * CO_H, CO_N = CO_R * CO_R, CO_NT = 256;
+
+__global__ void __launch_bounds__(CO_NT) mg_coarsen_kernel(MgLevel F, MgLevel C) {
+    __shared__ float sc[CO_N], sdx[CO_N], sdy[CO_N], st[CO_N];
+    const int wf = F.w, hf = F.h;
+    const int X0 = blockIdx.x * CO_S - CO_H, Y0 = blockIdx.y * CO_S - CO_H;  // even: local parity = global parity
+    for (int k = threadIdx.x; k < CO_N; k += CO_NT) {
+        const int gx = X0 + k % CO_R, gy = Y0 + k / CO_R;
+        float c = 1.0f, dx = 0.0f, dy = 0.0f, t = 0.0f;
+        if (gx >= 0 && gx < wf && gy >= 0 && gy < hf) {
+            const int i = gy * wf + gx;
+            c = F.c[i];
+            dx = F.dx[i];
+            dy = F.dy[i];
+            t = F.mask[i] ? 1.0f : 0.0f;
+        }
+        sc[k] = c;
+        sdx[k] = dx;
+        sdy[k] = dy;
+        st[k] = t;
+    }
+    __syncthreads();
+    // four half-sweeps, colour 0 first, over the region less its outermost ring (a cell's value is exact once it
+    // lies as many rings inside as half-sweeps were taken)
+    for (int sweep = 0; sweep < 4; sweep++) {
+        const int col = sweep & 1;
+        for (int k = threadIdx.x; k < CO_N / 2; k += CO_NT) {
+            const int ly = k / (CO_R / 2), lx = 2 * (k - ly * (CO_R / 2)) + ((ly + col) & 1);
+            if (lx < 1 || lx > CO_R - 2 || ly < 1 || ly > CO_R - 2) continue;
+            const int q = ly * CO_R + lx;
+            // a masked or outside cell has c = 1 and no couplings (nor do its neighbours towards it): it stays 0
+            const float dl = sdx[q - 1], dr = sdx[q], du = sdy[q - CO_R], dd = sdy[q];
+            const float num = dl * st[q - 1] + dr * st[q + 1] + du * st[q - CO_R] + dd * st[q + CO_R];
+            st[q] = num / (sc[q] + dl + dr + du + dd);
+        }
+        __syncthreads();
+    }
+    // each aggregate of the tile and of the two rings around it, scaled to a largest weight of 1 (an aggregate whose
+    // weights all vanished takes 1 on its system cells, as plain aggregation would)
+    constexpr int AG = (CO_S + 4) / 2;
+    for (int k = threadIdx.x; k < AG * AG; k += CO_NT) {
+        const int ay = k / AG, ax = k - ay * AG;
+        const int lx = CO_H - 2 + 2 * ax, ly = CO_H - 2 + 2 * ay;
+        const int q = ly * CO_R + lx;
+        const float m = fmaxf(fmaxf(st[q], st[q + 1]), fmaxf(st[q + CO_R], st[q + CO_R + 1]));
+        const int offs[4] = {0, 1, CO_R, CO_R + 1};
+        for (int e = 0; e < 4; e++) {
+            const int j = q + offs[e];
+            const int gx = X0 + lx + (e & 1), gy = Y0 + ly + (e >> 1);
+            const bool sys = gx >= 0 && gx < wf && gy >= 0 && gy < hf && F.mask[gy * wf + gx];
+            st[j] = !sys ? 0.0f : (m > 1e-30f ? st[j] / m : 1.0f);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < CO_S * CO_S; k += CO_NT) {
+        const int gx = X0 + CO_H + k % CO_S, gy = Y0 + CO_H + k / CO_S;
+        if (gx < wf && gy < hf) F.t[gy * wf + gx] = st[(k / CO_S + CO_H) * CO_R + k % CO_S + CO_H];
+    }
+    const int wc = C.w, hc = C.h;
+    for (int k = threadIdx.x; k < (CO_S / 2) * (CO_S / 2); k += CO_NT) {
+        const int cy = k / (CO_S / 2), cx = k - cy * (CO_S / 2);
+        const int X = blockIdx.x * (CO_S / 2) + cx, Y = blockIdx.y * (CO_S / 2) + cy;
+        if (X >= wc || Y >= hc) continue;
+        const int lx0 = CO_H + 2 * cx, ly0 = CO_H + 2 * cy;
+        double csum = 0.0;
+        bool any = false;
+        for (int b = 0; b < 2; b++)
+            for (int a = 0; a < 2; a++) {
+                const int q = (ly0 + b) * CO_R + lx0 + a;
+                const int gx = X0 + lx0 + a, gy = Y0 + ly0 + b;
+                if (gx >= wf || gy >= hf || !F.mask[gy * wf + gx]) continue;
+                any = true;
+                const double tj = st[q];
+                const double at = (double)sc[q] * tj + (double)sdx[q - 1] * (tj - st[q - 1]) +
+                                  (double)sdx[q] * (tj - st[q + 1]) + (double)sdy[q - CO_R] * (tj - st[q - CO_R]) +
+                                  (double)sdy[q] * (tj - st[q + CO_R]);
+                csum += tj * at;
+            }
+        double dxc = 0.0, dyc = 0.0;
+        if (X + 1 < wc)
+            for (int b = 0; b < 2; b++) {
+                const int q = (ly0 + b) * CO_R + lx0 + 1;
+                dxc += (double)st[q] * st[q + 1] * sdx[q];
+            }
+        if (Y + 1 < hc)
+            for (int a = 0; a < 2; a++) {
+                const int q = (ly0 + 1) * CO_R + lx0 + a;
+                dyc += (double)st[q] * st[q + CO_R] * sdy[q];
+            }
+        const size_t I = (size_t)Y * wc + X;
+        C.c[I] = any ? (float)csum : 1.0f;
+        C.dx[I] = any ? (float)dxc : 0.0f;
+        C.dy[I] = any ? (float)dyc : 0.0f;
+        C.mask[I] = any;
+    }
+}
+
 // One smoother on a big level, all NS half-sweeps of a tile in shared memory (the tile's halo as deep as the
 // half-sweeps, so the tile's result is exactly the global red-black sweeps'). PRE: from x = 0, red first, into L.x,
 // then the residual summed over each 2x2 aggregate into the coarse level's b (one more halo ring keeps the residual's
@@ -99,7 +203,7 @@ constexpr size_t smooth_smem() {
     return (size_t)RN * (PRE ? 6 : 5) * sizeof(float);
 }
 
-template <int NS, bool PRE, int SX, int SY, int NT, bool VEC>
+template <int NS, bool PRE, int SX, int SY, int NT, bool VEC, bool WT>
 __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, const float* __restrict__ xc,
                                                                     float omega, double* part, unsigned* counter,
                                                                     double* out) {
@@ -128,6 +232,7 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
                    dyu4 = b4, x4 = b4;
             float dxl = 0.0f;
             float2 xc2 = make_float2(0.f, 0.f);
+            float4 t4 = b4;
             const bool in = gy >= 0 && gy < h && gx0 >= 0 && gx0 < w;
             if (in) {
                 const size_t i = (size_t)gy * w + gx0;
@@ -139,19 +244,20 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
                 if (gx0 > 0) dxl = L.dx[i - 1];
                 if (!PRE) {
                     x4 = *reinterpret_cast<const float4*>(L.x + i);
+                    if constexpr (WT) t4 = *reinterpret_cast<const float4*>(L.t + i);
                     xc2 = *reinterpret_cast<const float2*>(xc + (size_t)(gy >> 1) * C.w + (gx0 >> 1));
                 }
             }
             const float bb[4] = {b4.x, b4.y, b4.z, b4.w}, cc[4] = {c4.x, c4.y, c4.z, c4.w};
             const float dxa[5] = {dxl, dx4.x, dx4.y, dx4.z, dx4.w}, dya[4] = {dy4.x, dy4.y, dy4.z, dy4.w};
             const float dyua[4] = {dyu4.x, dyu4.y, dyu4.z, dyu4.w}, xa[4] = {x4.x, x4.y, x4.z, x4.w};
-            const float xcv[2] = {xc2.x, xc2.y};
+            const float xcv[2] = {xc2.x, xc2.y}, ta[4] = {t4.x, t4.y, t4.z, t4.w};
 #pragma unroll
             for (int e = 0; e < 4; e++) {
                 const int lx = 4 * ch + e - OFF;
                 if (lx < 0 || lx >= RX) continue;
                 const float inv = in ? __fdividef(1.0f, cc[e] + dxa[e + 1] + dxa[e] + dya[e] + dyua[e]) : 0.0f;
-                const float x = (!PRE && in) ? xa[e] + omega * xcv[e >> 1] : 0.0f;
+                const float x = (!PRE && in) ? xa[e] + omega * (WT ? ta[e] : 1.0f) * xcv[e >> 1] : 0.0f;
                 const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
                 arr(A_X, col)[q] = x;
                 arr(A_B, col)[q] = bb[e];
@@ -177,7 +283,7 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
             dx = L.dx[i];
             dy = L.dy[i];
             const float dxl = gx > 0 ? L.dx[i - 1] : 0.0f, dyu = gy > 0 ? L.dy[i - w] : 0.0f;
-            if (!PRE) x = L.x[i] + omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
+            if (!PRE) x = L.x[i] + omega * (WT ? L.t[i] : 1.0f) * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
             inv = __fdividef(1.0f, c + dx + dxl + dy + dyu);  // the smoother's diagonal: an approximate reciprocal
         }
         const int col = (lx + ly) & 1, q = ly * HX + (lx >> 1);
@@ -240,7 +346,8 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
         }
     }
     if (PRE) {
-        // the coarse right-hand side: the residual, in difference form, summed over each aggregate of the tile
+        // the coarse right-hand side: the residual, in difference form, weighted by t and summed over each aggregate of
+        // the tile
         for (int k = tid; k < (SX / 2) * (SY / 2); k += NT) {
             const int cxl = k % (SX / 2), cyl = k / (SX / 2);
             const int X = (X0 + H) / 2 + cxl, Y = (Y0 + H) / 2 + cyl;
@@ -260,7 +367,12 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
                     ax += arr(A_DX, col)[q] * (xj - xo[right]);
                     ax += arr(A_DY, oth)[q - HX] * (xj - xo[q - HX]);
                     ax += arr(A_DY, col)[q] * (xj - xo[q + HX]);
-                    sum += arr(A_B, col)[q] - ax;
+                    if constexpr (WT) {
+                        const int gx = X0 + lx, gy = Y0 + ly;
+                        sum += (gx < w && gy < h ? L.t[gy * w + gx] : 0.0f) * (arr(A_B, col)[q] - ax);
+                    } else {
+                        sum += arr(A_B, col)[q] - ax;
+                    }
                 }
             C.b[(size_t)Y * C.w + X] = C.mask[(size_t)Y * C.w + X] ? sum : 0.0f;
         }
@@ -270,7 +382,7 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
 }
 
 // The coarsest level's operator inverted by Gauss-Jordan elimination in f64 in one CTA (n <= 64 cells), masked-out
-// cells as identity rows; stored f32. The operator is SPD and diagonally dominant, so no pivoting is needed.
+// cells as identity rows; stored f32. The operator is SPD, so no pivoting is needed.
 __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
     extern __shared__ double aug[];  // n x 2n
     const int w = C.w, h = C.h, n = w * h, m = 2 * n;
@@ -321,7 +433,8 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
 extern __shared__ __align__(16) unsigned char tail_smem_raw[];
 struct TailLevel {
     int w, h;
-    int c, dx, dy, b, x, inv;  // float offsets; inv: the inverse diagonal (0 on masked cells), formed once per launch
+    int c, dx, dy, b, x, inv, t;  // float offsets; inv: the inverse diagonal (0 on masked cells), formed once per
+                                  // launch; t: the weights towards the next coarser level
     int m;                     // byte offset of the mask
 };
 __device__ __forceinline__ float* tsf() { return reinterpret_cast<float*>(tail_smem_raw); }
@@ -351,7 +464,7 @@ __device__ __forceinline__ void tail_sweep(const TailLevel T, int color) {
 
 __device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel C) {
     float* f = tsf();
-    const float *fc = f + F.c, *fdx = f + F.dx, *fdy = f + F.dy, *fb = f + F.b, *fx = f + F.x;
+    const float *fc = f + F.c, *fdx = f + F.dx, *fdy = f + F.dy, *fb = f + F.b, *fx = f + F.x, *ft = f + F.t;
     const uint8_t* fm = tail_smem_raw + F.m;
     const uint8_t* cm = tail_smem_raw + C.m;
     float *cb = f + C.b, *cx = f + C.x;
@@ -372,7 +485,7 @@ __device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel
                     if (x + 1 < F.w) ax += fdx[j] * (xj - fx[j + 1]);
                     if (y > 0) ax += fdy[j - F.w] * (xj - fx[j - F.w]);
                     if (y + 1 < F.h) ax += fdy[j] * (xj - fx[j + F.w]);
-                    sum += fb[j] - ax;
+                    sum += ft[j] * (fb[j] - ax);
                 }
             cb[I] = cm[I] ? sum : 0.0f;
             cx[I] = 0.0f;
@@ -396,8 +509,9 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
             T[l].b = off + 3 * n;
             T[l].x = off + 4 * n;
             T[l].inv = off + 5 * n;
+            T[l].t = off + 6 * n;
         }
-        off += 6 * n;
+        off += 7 * n;
     }
     const int nc = A.L[A.nl - 1].w * A.L[A.nl - 1].h;
     float* sinv = f + off;  // the coarsest level's inverse, nc x nc
@@ -418,6 +532,7 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
             f[Tl.dy + i] = A.L[l].dy[i];
             tail_smem_raw[Tl.m + i] = A.L[l].mask[i];
             f[Tl.x + i] = 0.0f;
+            f[Tl.t + i] = l + 1 < A.nl ? (A.L[l].t ? A.L[l].t[i] : 1.0f) : 0.0f;
             if (l == A.t) f[Tl.b + i] = A.L[l].b[i];
         }
     }
@@ -463,7 +578,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
             for (int y = ty; y < F.h; y += TAIL_ROWS)
                 for (int x = tx; x < F.w; x += 32) {
                     const int i = y * F.w + x;
-                    if (tail_smem_raw[F.m + i]) f[F.x + i] += A.omega * f[Cs.x + (y >> 1) * Cs.w + (x >> 1)];
+                    if (tail_smem_raw[F.m + i])
+                        f[F.x + i] += A.omega * f[F.t + i] * f[Cs.x + (y >> 1) * Cs.w + (x >> 1)];
                 }
         }
         __syncthreads();
@@ -496,25 +612,36 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
 
 size_t tail_smem(const Multigrid& M) {
     size_t s = 0;
-    for (int l = M.tail; l < M.nlevels; l++) s += (size_t)M.L[l].w * M.L[l].h * (6 * sizeof(float) + 1);
+    for (int l = M.tail; l < M.nlevels; l++) s += (size_t)M.L[l].w * M.L[l].h * (7 * sizeof(float) + 1);
     const size_t nc = (size_t)M.L[M.nlevels - 1].w * M.L[M.nlevels - 1].h;
     s += sizeof(float) * nc * nc;
     return (s + 15) & ~(size_t)15;
 }
 
+template <int NS, bool PRE, int SX, int SY, int NT, bool VEC, bool WT>
+void launch_one(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
+                double* out, cudaStream_t s) {
+    const dim3 grid(div_up(L.w, SX), div_up(L.h, SY));
+    mg_smooth_kernel<NS, PRE, SX, SY, NT, VEC, WT><<<grid, NT, smooth_smem<NS, PRE, SX, SY>(), s>>>(
+        L, C, xc, omega, part, counter, out);
+}
+
 template <int NS, bool PRE, int SX, int SY, int NT>
 void launch_smooth_t(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
                      double* out, cudaStream_t s) {
-    dim3 grid(div_up(L.w, SX), div_up(L.h, SY));
     // 16-byte rows (and 8-byte coarse pairs) stay aligned; the pre-smoother's odd halo would load 8 % more columns, and
-    // measured slower, so it keeps the per-cell loads
-    const bool vec = !PRE && L.w % 4 == 0 && C.w % 2 == 0;
-    if (vec)
-        mg_smooth_kernel<NS, PRE, SX, SY, NT, true><<<grid, NT, smooth_smem<NS, PRE, SX, SY>(), s>>>(
-            L, C, xc, omega, part, counter, out);
-    else
-        mg_smooth_kernel<NS, PRE, SX, SY, NT, false><<<grid, NT, smooth_smem<NS, PRE, SX, SY>(), s>>>(
-            L, C, xc, omega, part, counter, out);
+    // measured slower, so it keeps the per-cell loads. Level 0 has no weights (its kernels read none).
+    const bool wt = L.t != nullptr;
+    if constexpr (!PRE) {
+        if (L.w % 4 == 0 && C.w % 2 == 0) {
+            if (wt) launch_one<NS, PRE, SX, SY, NT, true, true>(L, C, xc, omega, part, counter, out, s);
+            else launch_one<NS, PRE, SX, SY, NT, true, false>(L, C, xc, omega, part, counter, out, s);
+            sr_note_launch();
+            return;
+        }
+    }
+    if (wt) launch_one<NS, PRE, SX, SY, NT, false, true>(L, C, xc, omega, part, counter, out, s);
+    else launch_one<NS, PRE, SX, SY, NT, false, false>(L, C, xc, omega, part, counter, out, s);
     sr_note_launch();
 }
 
@@ -543,16 +670,20 @@ void smooth(int nu, bool pre, const MgLevel& L, const MgLevel& C, const float* x
     }
 }
 
+template <int NS, bool PRE, int SX, int SY, int NT, bool VEC, bool WT>
+void set_attribute_one() {
+    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, PRE, SX, SY, NT, VEC, WT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, PRE, SX, SY>()));
+}
+
 template <int NS, int SX, int SY, int NT>
 void set_attributes_tile() {
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true, SX, SY, NT, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, true, SX, SY>()));
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false, SX, SY, NT, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, false, SX, SY>()));
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, true, SX, SY, NT, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, true, SX, SY>()));
-    SR_CUDA_TRY(cudaFuncSetAttribute(mg_smooth_kernel<NS, false, SX, SY, NT, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smooth_smem<NS, false, SX, SY>()));
+    set_attribute_one<NS, true, SX, SY, NT, false, false>();
+    set_attribute_one<NS, true, SX, SY, NT, false, true>();
+    set_attribute_one<NS, false, SX, SY, NT, false, false>();
+    set_attribute_one<NS, false, SX, SY, NT, false, true>();
+    set_attribute_one<NS, false, SX, SY, NT, true, false>();
+    set_attribute_one<NS, false, SX, SY, NT, true, true>();
 }
 
 template <int NS>
@@ -593,6 +724,7 @@ void Multigrid::create(int w, int h, int pre_, int post_) {
         SR_CUDA_TRY(cudaMalloc(&L.mask, n));
         SR_CUDA_TRY(cudaMalloc(&L.x, n * sizeof(float)));
         if (nlevels > 0) {
+            SR_CUDA_TRY(cudaMalloc(&L.t, n * sizeof(float)));
             SR_CUDA_TRY(cudaMalloc(&L.b, n * sizeof(float)));
             SR_CUDA_TRY(cudaMalloc(&L.x2, n * sizeof(float)));
         }
@@ -624,6 +756,7 @@ void Multigrid::destroy() {
         cudaFree(L[l].mask);
         cudaFree(L[l].x);
         if (l > 0) {
+            cudaFree(L[l].t);
             cudaFree(L[l].b);
             cudaFree(L[l].x2);
         }
@@ -636,7 +769,8 @@ void Multigrid::destroy() {
 
 size_t Multigrid::bytes() const {
     size_t s = 0;
-    for (int l = 0; l < nlevels; l++) s += (size_t)L[l].w * L[l].h * (l ? 6 * sizeof(float) + 1 : 4 * sizeof(float) + 1);
+    for (int l = 0; l < nlevels; l++)
+        s += (size_t)L[l].w * L[l].h * (l ? 7 * sizeof(float) + 1 : 4 * sizeof(float) + 1);
     return s;
 }
 
@@ -645,70 +779,27 @@ void Multigrid::set_couplings(const double* kx, const double* ky, const uint8_t*
     sr_note_launch();
 }
 
-// The smoother tile of each level below 0 (level 0 keeps the CTA-count rule, which bounds its grid-sum partials) chosen
-// by timing: the big and the small tile, pre- and post-smoother, three launches each, on the level's current operator.
-// Choices are kept per level size for the process (a batch's worlds of one size tune once).
-void Multigrid::autotune(cudaStream_t s) {
-    static std::mutex mu;
-    static std::map<std::pair<int, int>, int> chosen;
-    tuned = true;
-    for (int l = 1; l < tail; l++) {
-        const std::pair<int, int> key(L[l].w, L[l].h);
-        {
-            std::lock_guard<std::mutex> g(mu);
-            auto it = chosen.find(key);
-            if (it != chosen.end()) {
-                tile[l] = it->second;
-                continue;
-            }
-        }
-        cudaEvent_t a, b;
-        SR_CUDA_TRY(cudaEventCreate(&a));
-        SR_CUDA_TRY(cudaEventCreate(&b));
-        float best = 0.0f;
-        int pick = small_tiles(L[l]) ? 1 : 0;
-        for (int cand = 0; cand < 2; cand++) {
-            float total = 0.0f;
-            for (int rep = 0; rep < 4; rep++) {  // the first launch of each warms up
-                SR_CUDA_TRY(cudaEventRecord(a, s));
-                smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s, cand);
-                smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, nullptr, nullptr, nullptr, s, cand);
-                SR_CUDA_TRY(cudaEventRecord(b, s));
-                SR_CUDA_TRY(cudaEventSynchronize(b));
-                float t = 0.0f;
-                SR_CUDA_TRY(cudaEventElapsedTime(&t, a, b));
-                if (rep > 0) total += t;
-            }
-            if (cand == 0 || total < best) {
-                best = total;
-                pick = cand;
-            }
-        }
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
-        tile[l] = pick;
-        std::lock_guard<std::mutex> g(mu);
-        chosen[key] = pick;
-    }
-}
-
 void Multigrid::coarsen(cudaStream_t s) {
     for (int l = 1; l < nlevels; l++) {
-        mg_coarsen_kernel<<<grid_for((size_t)L[l].w * L[l].h), 256, 0, s>>>(L[l - 1], L[l]);
+        if (l == 1) {
+            mg_aggregate_kernel<<<grid_for((size_t)L[1].w * L[1].h), 256, 0, s>>>(L[0], L[1]);
+        } else {
+            const dim3 grid(div_up(L[l - 1].w, CO_S), div_up(L[l - 1].h, CO_S));
+            mg_coarsen_kernel<<<grid, CO_NT, 0, s>>>(L[l - 1], L[l]);
+        }
         sr_note_launch();
     }
     const MgLevel& C = L[nlevels - 1];
     const size_t nc = (size_t)C.w * C.h;
     mg_coarse_inverse_kernel<<<1, 1024, nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
     sr_note_launch();
-    if (!tuned) autotune(s);
 }
 
 void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter, double* rz_out, cudaStream_t s) {
     L[0].b = const_cast<float*>(r);
     L[0].x2 = z;
     for (int l = 0; l < tail; l++)
-        smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s, tile[l]);
+        smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s);
     TailArgs T;
     T.coarse_inv = coarse_inv;
     T.t = tail;
@@ -722,7 +813,7 @@ void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter,
     sr_note_launch();
     for (int l = tail - 1; l >= 0; l--)
         smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, l == 0 ? part : nullptr, l == 0 ? counter : nullptr,
-               l == 0 ? rz_out : nullptr, s, tile[l]);
+               l == 0 ? rz_out : nullptr, s);
 }
 
 void Multigrid::time_level0(int reps, void* flush, size_t flush_bytes, cudaStream_t s, double* pre_ms,
@@ -738,9 +829,9 @@ void Multigrid::time_level0(int reps, void* flush, size_t flush_bytes, cudaStrea
             SR_CUDA_TRY(cudaMemsetAsync(flush, k & 0xff, flush_bytes, s));
             SR_CUDA_TRY(cudaEventRecord(a, s));
             if (which == 0)
-                smooth(pre, true, L[0], L[1], nullptr, omega, nullptr, nullptr, nullptr, s, tile[0]);
+                smooth(pre, true, L[0], L[1], nullptr, omega, nullptr, nullptr, nullptr, s);
             else
-                smooth(post, false, L[0], L[1], L[1].x2, omega, nullptr, nullptr, nullptr, s, tile[0]);
+                smooth(post, false, L[0], L[1], L[1].x2, omega, nullptr, nullptr, nullptr, s);
             SR_CUDA_TRY(cudaEventRecord(b, s));
             SR_CUDA_TRY(cudaEventSynchronize(b));
             float t = 0.0f;
