@@ -382,9 +382,12 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
 }
 
 // The coarsest level's operator inverted by Gauss-Jordan elimination in f64 in one CTA (n <= 64 cells), masked-out
-// cells as identity rows; stored f32. The operator is SPD, so no pivoting is needed.
+// cells as identity rows; stored f32. The operator is SPD, so no pivoting is needed. The augmented matrix [A | I] is
+// kept twice and each elimination step reads one copy and writes the other, so a step is one pass and one barrier;
+// at step p only columns p .. n + p change (to the left the pivot row is already 0, to the right of n + p it is still
+// 0: untouched identity columns, the same in both copies).
 __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
-    extern __shared__ double aug[];  // n x 2n
+    extern __shared__ double aug[];  // two n x 2n copies
     const int w = C.w, h = C.h, n = w * h, m = 2 * n;
     for (int k = threadIdx.x; k < n * m; k += blockDim.x) {
         const int i = k / m, j = k % m;
@@ -404,27 +407,23 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
             else if (yi + 1 < h && j == i + w) v = -dd;
         }
         aug[k] = v;
+        aug[n * m + k] = v;
     }
     __syncthreads();
-    // at step p only columns p .. n + p can change: to the left the pivot row is already 0 (eliminated columns), to the
-    // right of n + p it is still 0 (the untouched identity columns)
     const int na = n + 1;
     for (int p = 0; p < n; p++) {
-        const double piv = aug[p * m + p];
-        __syncthreads();
-        for (int j = p + threadIdx.x; j <= n + p; j += blockDim.x) aug[p * m + j] /= piv;
-        __syncthreads();
+        const double* src = aug + (p & 1) * n * m;
+        double* dst = aug + ((p + 1) & 1) * n * m;
+        const double rpiv = 1.0 / src[p * m + p];
         for (int k = threadIdx.x; k < n * na; k += blockDim.x) {
             const int i = k / na, j = p + k % na;
-            if (i != p && j != p) aug[i * m + j] -= aug[i * m + p] * aug[p * m + j];
+            const double apj = src[p * m + j] * rpiv;
+            dst[i * m + j] = i == p ? apj : src[i * m + j] - src[i * m + p] * apj;
         }
         __syncthreads();
-        // column p of the other rows, read as the elimination factor above, becomes 0
-        for (int i = threadIdx.x; i < n; i += blockDim.x)
-            if (i != p) aug[i * m + p] = 0.0;
-        __syncthreads();
     }
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) inv[k] = (float)aug[(k / n) * m + n + (k % n)];
+    const double* fin = aug + (n & 1) * n * m;
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) inv[k] = (float)fin[(k / n) * m + n + (k % n)];
 }
 
 // ---- the coarse tail: every level from t on, inside one CTA
@@ -742,7 +741,7 @@ void Multigrid::create(int w, int h, int pre_, int post_) {
     SR_REQUIRE(nc <= 64, "the coarsest level holds more than 64 cells");
     SR_CUDA_TRY(cudaMalloc(&coarse_inv, sizeof(float) * nc * nc));
     SR_CUDA_TRY(cudaFuncSetAttribute(mg_coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(nc * 2 * nc * sizeof(double))));
+                                     (int)(2 * nc * 2 * nc * sizeof(double))));
     set_attributes_ns<2>();
     set_attributes_ns<4>();
     set_attributes_ns<6>();
@@ -791,7 +790,7 @@ void Multigrid::coarsen(cudaStream_t s) {
     }
     const MgLevel& C = L[nlevels - 1];
     const size_t nc = (size_t)C.w * C.h;
-    mg_coarse_inverse_kernel<<<1, 1024, nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
+    mg_coarse_inverse_kernel<<<1, 1024, 2 * nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
     sr_note_launch();
 }
 
