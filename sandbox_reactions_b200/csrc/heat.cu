@@ -886,6 +886,7 @@ struct SolveResult {
     bool fallback = false;  // the learned preconditioner stalled and MG-PCG finished
 };
 
+constexpr double kFirstPassTol = 0.1;  // the first Newton pass's relative residual (and the loosest any pass asks)
 constexpr int kStallRounds = 24;  // learned: rounds after which a solve that has not gained 100x falls back
 
 // PCG on A32 e = r32 from e = 0 to a residual reduction `eta` or `max_it` rounds. Returns the rounds, -1 on a
@@ -1179,10 +1180,12 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     }
     uint32_t passes = 0, rounds = 0;
     bool converged = false;
-    // Inexact Newton: a pass's solve is asked for 1e-2 of the last pass's relative heat moved (at most 1e-4), never
-    // less than solve_tol; the passes end only on a pass solved to solve_tol.
+    // Inexact Newton: a pass's solve is asked for the last pass's relative heat moved (the first pass for
+    // kFirstPassTol), never more than kFirstPassTol nor less than solve_tol; the passes end only on a pass solved to
+    // solve_tol. Loose early passes cost fewer rounds in all than accurate ones: each pass's system is rebuilt at the
+    // new iterate anyway, and the last pass meets the same tolerances.
     const double tol = H->cfg.solve_tol;
-    double pass_tol = std::max(tol, 1e-4);
+    double pass_tol = std::max(tol, kFirstPassTol);
     while (passes < H->max_passes && rounds < H->max_rounds) {
         passes++;
         build_system(H, dt, s);
@@ -1201,7 +1204,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
             converged = true;
             break;
         }
-        pass_tol = std::max(tol, std::min(1e-4, 1e-2 * rel_moved));
+        pass_tol = std::max(tol, std::min(kFirstPassTol, rel_moved));
     }
     R.passes = passes;
     R.rounds = rounds;
