@@ -22,8 +22,8 @@ namespace {
 constexpr int RED_THREADS = 256;
 constexpr int MAX_PART = 1184;    // most CTAs of a grid-stride heat kernel: one wave (148 SMs x 8), few partials to sum
 constexpr int PART_CAP = 16384;   // partials per reduced value (the level-0 smoother's CTAs included)
-enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1, S_ZRO, S_MGRZ, S_BETA,
-            S_MOVED, S_VIOL, S_RAD, S_GAIN, S_HELD, S_COUNT };
+enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_MOVED, S_VIOL, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1,
+            S_ZRO, S_MGRZ, S_BETA, S_RAD, S_GAIN, S_HELD, S_COUNT };
 
 // Where a kernel's grid sum goes: the partials buffer, the ticket counter and the device scalar(s).
 struct Red {
@@ -561,27 +561,39 @@ __global__ void correction_kernel(size_t n, const uint8_t* __restrict__ gas, con
         if (gas[i]) x[i] += scale * (double)e[i];
 }
 
-// The pass's update (heat.rs:494-509): u >= u_vac, T within a factor 2; partials of Σ C|ΔT| and of the cells moved
-// by more than newton_cell of their T.
-__global__ void newton_update_kernel(HeatConst K, double cell_tol, const uint8_t* __restrict__ gas,
-                                     const double* __restrict__ C, const double* __restrict__ x, double* t, double* u,
-                                     Red R) {
+// The pass's update (heat.rs:494-509: u >= u_vac, T within a factor 2) and the next pass's system at the new iterate
+// (as heat_system_kernel builds it) in one sweep over the cells; partials of Σ C|ΔT|, the cells moved by more than
+// newton_cell of their T, Σ c_i u² and Σ (C/Δt) T² (four consecutive slots from S_MOVED). When the passes end here
+// the system goes unused.
+__global__ void newton_system_kernel(HeatConst K, double cell_tol, double dt, const uint8_t* __restrict__ gas,
+                                     const double* __restrict__ C, const double* __restrict__ t0,
+                                     const double* __restrict__ kvac, double* t, double* u, double* x, double* c64,
+                                     double* rhs, float* c0, Red R) {
     const size_t n = (size_t)K.w * K.h;
     const double u_vac = u_of(K, K.t_floor);
-    double moved = 0.0, viol = 0.0;
+    double moved = 0.0, viol = 0.0, ub = 0.0, tb = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        if (!gas[i]) continue;
+        if (!gas[i]) continue;  // the system's masked rows (c = 1, b = 0, x = 0) are already in place
         const double ti = t[i];
         double nx = t_of(K, fmax(x[i], u_vac));
         nx = fmin(fmax(nx, 0.5 * ti), 2.0 * ti);
         const double d = fabs(nx - ti);
         moved += C[i] * d;
         if (!(d <= cell_tol * ti)) viol += 1.0;
+        const double un = u_of(K, nx);
         t[i] = nx;
-        u[i] = u_of(K, nx);
+        u[i] = un;
+        const double heat = C[i] / dt;
+        const double ci = heat * dt_du(K, nx);
+        c64[i] = ci + kvac[i];
+        rhs[i] = ci * un - heat * (nx - t0[i]) + kvac[i] * u_vac;
+        c0[i] = (float)(ci + kvac[i]);
+        x[i] = un;
+        ub += ci * un * un;
+        tb += heat * nx * nx;
     }
-    const double v[2] = {moved, viol};
-    grid_sum_last<2>(v, R.part, R.counter, R.out);
+    const double v[4] = {moved, viol, ub, tb};
+    grid_sum_last<4>(v, R.part, R.counter, R.out);
 }
 
 // F = -k (v_b - v_a) at every face (heat.rs:338-361), v = u on gas cells, u_vac elsewhere; FP32 out.
@@ -887,12 +899,14 @@ struct SolveResult {
 };
 
 constexpr double kFirstPassTol = 0.1;  // the first Newton pass's relative residual (and the loosest any pass asks)
+constexpr double kTrustedPassTol = 1e-5;  // passes this loose end on their FP32 solve's own test
 constexpr int kStallRounds = 24;  // learned: rounds after which a solve that has not gained 100x falls back
 
 // PCG on A32 e = r32 from e = 0 to a residual reduction `eta` or `max_it` rounds. Returns the rounds, -1 on a
 // breakdown (a non-positive or non-finite curvature), or with the learned preconditioner -2 - rounds when it stalls
 // (a breakdown, or less than a 100x reduction after kStallRounds): plain MG-PCG then takes over.
-int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStream_t s) {
+int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStream_t s, bool* reached = nullptr) {
+    if (reached) *reached = false;
     precondition(H, precond, S_RZ0, s);
     if (precond == SR_PRECOND_LEARNED) {  // flexible CG forms its direction at the end of a round
         pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, -1, S_RZ0, H->z32, H->p32);
@@ -912,7 +926,10 @@ int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStrea
             H->read(S_PQ, 2, s);  // S_PQ, S_RRI
             const double pq = H->hscal[S_PQ], rr = H->hscal[S_RRI];
             if (!(pq > 0.0) || !isfinite(pq) || !isfinite(rr)) return precond == SR_PRECOND_LEARNED ? -2 - it : -1;
-            if (rr <= eta * eta * rr0) break;
+            if (rr <= eta * eta * rr0) {
+                if (reached) *reached = true;
+                break;
+            }
             if (precond == SR_PRECOND_LEARNED && it >= kStallRounds && rr > 1e-4 * rr0) return -2 - it;
             // after the first three rounds, the next check one round before the rate seen so far (the geometric mean
             // per round) reaches the target: each check costs a host round trip, each round past convergence a V-cycle
@@ -955,7 +972,8 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->red(S_R32));
         sr_note_launch();
         const double eta = std::min(0.5, std::max(H->inner_floor, 0.5 / worst));
-        int it = inner_pcg(H, precond, eta, max_rounds - R.rounds, s);
+        bool reached = false;
+        int it = inner_pcg(H, precond, eta, max_rounds - R.rounds, s, &reached);
         if (it <= -2) {  // the learned preconditioner stalled: its inner solve is dropped, MG-PCG restarts from x
             R.rounds += -2 - it;
             R.fallback = true;
@@ -971,6 +989,12 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         R.refinements++;
         correction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->gas, H->e32, scale, H->x);
         sr_note_launch();
+        // an intermediate Newton pass (its tolerance far above the FP32 solve's floor) trusts the FP32 solve that
+        // reached its reduction: the next pass starts from a fresh residual anyway; the final pass is always verified
+        if (reached && tol >= kTrustedPassTol) {
+            R.rel *= eta;
+            return R;
+        }
     }
     return R;
 }
@@ -1186,25 +1210,27 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     // new iterate anyway, and the last pass meets the same tolerances.
     const double tol = H->cfg.solve_tol;
     double pass_tol = std::max(tol, kFirstPassTol);
+    build_system(H, dt, s);
     while (passes < H->max_passes && rounds < H->max_rounds) {
         passes++;
-        build_system(H, dt, s);
         SolveResult S = solve_pass(H, H->precond, pass_tol, (int)(H->max_rounds - rounds), dt, s);
         rounds += (uint32_t)S.rounds;
         R.refinements += (uint32_t)S.refinements;
         R.rel_residual = S.rel;
         if (S.fallback) R.fallback_used = 1;
         if (!S.ok) break;
-        newton_update_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->cfg.newton_cell, H->gas, H->C, H->x, H->t, H->u,
-                                                              H->red(S_MOVED));
+        newton_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->cfg.newton_cell, dt, H->gas, H->C, H->t0,
+                                                              H->kvac, H->t, H->u, H->x, H->c64, H->rhs,
+                                                              H->mg.L[0].c, H->red(S_MOVED));
         sr_note_launch();
-        H->read(S_MOVED, 2, s);
+        H->read(S_MOVED, 4, s);  // moved, violations, and the next system's two bounds
         const double rel_moved = heat0 > 0.0 ? H->hscal[S_MOVED] / heat0 : 0.0;
         if (rel_moved <= H->cfg.newton_heat && H->hscal[S_VIOL] == 0.0 && pass_tol <= tol) {
             converged = true;
             break;
         }
         pass_tol = std::max(tol, std::min(kFirstPassTol, rel_moved));
+        H->mg.coarsen(s);  // the next pass's coarse levels (its level-0 c is in place)
     }
     R.passes = passes;
     R.rounds = rounds;
