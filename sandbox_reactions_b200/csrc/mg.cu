@@ -646,13 +646,35 @@ void launch_smooth_t(const MgLevel& L, const MgLevel& C, const float* xc, float 
 
 bool small_tiles(const MgLevel& L) { return (size_t)div_up(L.w, BIG_SX) * div_up(L.h, BIG_SY) < 2 * 148; }
 
+// A smoother's tile height: of the even heights from SY_MAX down to SY_MAX - 6, the one with the most output cells per
+// sweep slot (a half-sweep gives each thread ceil(cells of one colour in the halo'd tile / NT) slots; the last slot
+// round should be nearly full, or most threads wait at its barrier).
+template <int NS, bool PRE, int SX, int SY_MAX, int NT>
+constexpr int tile_sy() {
+    constexpr int H = PRE ? NS + 1 : NS;
+    int best = SY_MAX;
+    double best_rate = 0.0;
+    for (int sy = SY_MAX; sy >= SY_MAX - 6; sy -= 2) {
+        const int hn = (SX + 2 * H) / 2 * (sy + 2 * H);
+        const int slots = (hn + NT - 1) / NT;
+        const double rate = (double)(SX * sy) / slots;
+        if (rate > best_rate) {
+            best_rate = rate;
+            best = sy;
+        }
+    }
+    return best;
+}
+
 template <int NS, bool PRE>
 void launch_smooth(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
                    double* out, int tile, cudaStream_t s) {
     if (tile < 0 ? small_tiles(L) : tile == 1)
-        launch_smooth_t<NS, PRE, SMALL_SX, SMALL_SY, SMALL_NT>(L, C, xc, omega, part, counter, out, s);
+        launch_smooth_t<NS, PRE, SMALL_SX, tile_sy<NS, PRE, SMALL_SX, SMALL_SY, SMALL_NT>(), SMALL_NT>(
+            L, C, xc, omega, part, counter, out, s);
     else
-        launch_smooth_t<NS, PRE, BIG_SX, BIG_SY, BIG_NT>(L, C, xc, omega, part, counter, out, s);
+        launch_smooth_t<NS, PRE, BIG_SX, tile_sy<NS, PRE, BIG_SX, BIG_SY, BIG_NT>(), BIG_NT>(L, C, xc, omega, part,
+                                                                                           counter, out, s);
 }
 
 // `tile`: 0 the big tile, 1 the small one, -1 by the CTA-count rule (small_tiles).
@@ -677,12 +699,13 @@ void set_attribute_one() {
 
 template <int NS, int SX, int SY, int NT>
 void set_attributes_tile() {
-    set_attribute_one<NS, true, SX, SY, NT, false, false>();
-    set_attribute_one<NS, true, SX, SY, NT, false, true>();
-    set_attribute_one<NS, false, SX, SY, NT, false, false>();
-    set_attribute_one<NS, false, SX, SY, NT, false, true>();
-    set_attribute_one<NS, false, SX, SY, NT, true, false>();
-    set_attribute_one<NS, false, SX, SY, NT, true, true>();
+    constexpr int PSY = tile_sy<NS, true, SX, SY, NT>(), QSY = tile_sy<NS, false, SX, SY, NT>();
+    set_attribute_one<NS, true, SX, PSY, NT, false, false>();
+    set_attribute_one<NS, true, SX, PSY, NT, false, true>();
+    set_attribute_one<NS, false, SX, QSY, NT, false, false>();
+    set_attribute_one<NS, false, SX, QSY, NT, false, true>();
+    set_attribute_one<NS, false, SX, QSY, NT, true, false>();
+    set_attribute_one<NS, false, SX, QSY, NT, true, true>();
 }
 
 template <int NS>
@@ -702,8 +725,9 @@ size_t mg_smooth_ctas(int w, int h) {
     MgLevel L;
     L.w = w;
     L.h = h;
-    return small_tiles(L) ? (size_t)div_up(w, SMALL_SX) * div_up(h, SMALL_SY)
-                          : (size_t)div_up(w, BIG_SX) * div_up(h, BIG_SY);
+    // a bound: the shortest tile tile_sy can pick
+    return small_tiles(L) ? (size_t)div_up(w, SMALL_SX) * div_up(h, SMALL_SY - 6)
+                          : (size_t)div_up(w, BIG_SX) * div_up(h, BIG_SY - 6);
 }
 
 void Multigrid::create(int w, int h, int pre_, int post_) {

@@ -32,7 +32,7 @@ struct MgLevel {
     float* t = nullptr;   // the cell's weight in its aggregate's basis function (null: 1, level 0)
 };
 
-// CTAs of one smoother launch on a w x h level (each writes one grid-sum partial at level 0).
+// At most this many CTAs in one smoother launch on a w x h level (each writes one grid-sum partial at level 0).
 size_t mg_smooth_ctas(int w, int h);
 
 struct Multigrid {
