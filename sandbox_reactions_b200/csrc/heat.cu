@@ -569,28 +569,48 @@ __global__ void newton_system_kernel(HeatConst K, double cell_tol, double dt, co
                                      const double* __restrict__ C, const double* __restrict__ t0,
                                      const double* __restrict__ kvac, double* t, double* u, double* x, double* c64,
                                      double* rhs, float* c0, Red R) {
-    const size_t n = (size_t)K.w * K.h;
+    const size_t n = (size_t)K.w * K.h, stride = (size_t)gridDim.x * blockDim.x;
     const double u_vac = u_of(K, K.t_floor);
     double moved = 0.0, viol = 0.0, ub = 0.0, tb = 0.0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        if (!gas[i]) continue;  // the system's masked rows (c = 1, b = 0, x = 0) are already in place
-        const double ti = t[i];
-        double nx = t_of(K, fmax(x[i], u_vac));
-        nx = fmin(fmax(nx, 0.5 * ti), 2.0 * ti);
-        const double d = fabs(nx - ti);
-        moved += C[i] * d;
-        if (!(d <= cell_tol * ti)) viol += 1.0;
-        const double un = u_of(K, nx);
-        t[i] = nx;
-        u[i] = un;
-        const double heat = C[i] / dt;
-        const double ci = heat * dt_du(K, nx);
-        c64[i] = ci + kvac[i];
-        rhs[i] = ci * un - heat * (nx - t0[i]) + kvac[i] * u_vac;
-        c0[i] = (float)(ci + kvac[i]);
-        x[i] = un;
-        ub += ci * un * un;
-        tb += heat * nx * nx;
+    // two cells a grid stride apart per iteration, all loads issued before the arithmetic
+    for (size_t base = (size_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += 2 * stride) {
+        const size_t i2 = base + stride;
+        const bool g1 = gas[base], g2 = i2 < n && gas[i2];
+        double tv[2], xv[2], Cv[2], t0v[2], kv[2];
+        tv[0] = t[base];
+        xv[0] = x[base];
+        Cv[0] = C[base];
+        t0v[0] = t0[base];
+        kv[0] = kvac[base];
+        if (i2 < n) {
+            tv[1] = t[i2];
+            xv[1] = x[i2];
+            Cv[1] = C[i2];
+            t0v[1] = t0[i2];
+            kv[1] = kvac[i2];
+        }
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const size_t i = e ? i2 : base;
+            if (!(e ? g2 : g1)) continue;  // the system's masked rows (c = 1, b = 0, x = 0) are already in place
+            const double ti = tv[e];
+            double nx = t_of(K, fmax(xv[e], u_vac));
+            nx = fmin(fmax(nx, 0.5 * ti), 2.0 * ti);
+            const double d = fabs(nx - ti);
+            moved += Cv[e] * d;
+            if (!(d <= cell_tol * ti)) viol += 1.0;
+            const double un = u_of(K, nx);
+            t[i] = nx;
+            u[i] = un;
+            const double heat = Cv[e] / dt;
+            const double ci = heat * dt_du(K, nx);
+            c64[i] = ci + kv[e];
+            rhs[i] = ci * un - heat * (nx - t0v[e]) + kv[e] * u_vac;
+            c0[i] = (float)(ci + kv[e]);
+            x[i] = un;
+            ub += ci * un * un;
+            tb += heat * nx * nx;
+        }
     }
     const double v[4] = {moved, viol, ub, tb};
     grid_sum_last<4>(v, R.part, R.counter, R.out);

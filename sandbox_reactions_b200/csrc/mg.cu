@@ -88,18 +88,22 @@ constexpr int CO_S = 32, CO_H = 6, CO_R = CO_S + 2 * CO_H, CO_N = CO_R * CO_R, C
 
 __global__ void __launch_bounds__(CO_NT) mg_coarsen_kernel(MgLevel F, MgLevel C) {
     __shared__ float sc[CO_N], sdx[CO_N], sdy[CO_N], st[CO_N];
+    __shared__ uint8_t sm[CO_N];
     const int wf = F.w, hf = F.h;
     const int X0 = blockIdx.x * CO_S - CO_H, Y0 = blockIdx.y * CO_S - CO_H;  // even: local parity = global parity
     for (int k = threadIdx.x; k < CO_N; k += CO_NT) {
         const int gx = X0 + k % CO_R, gy = Y0 + k / CO_R;
         float c = 1.0f, dx = 0.0f, dy = 0.0f, t = 0.0f;
+        uint8_t m = 0;
         if (gx >= 0 && gx < wf && gy >= 0 && gy < hf) {
             const int i = gy * wf + gx;
             c = F.c[i];
             dx = F.dx[i];
             dy = F.dy[i];
-            t = F.mask[i] ? 1.0f : 0.0f;
+            m = F.mask[i];
+            t = m ? 1.0f : 0.0f;
         }
+        sm[k] = m;
         sc[k] = c;
         sdx[k] = dx;
         sdy[k] = dy;
@@ -132,9 +136,7 @@ __global__ void __launch_bounds__(CO_NT) mg_coarsen_kernel(MgLevel F, MgLevel C)
         const int offs[4] = {0, 1, CO_R, CO_R + 1};
         for (int e = 0; e < 4; e++) {
             const int j = q + offs[e];
-            const int gx = X0 + lx + (e & 1), gy = Y0 + ly + (e >> 1);
-            const bool sys = gx >= 0 && gx < wf && gy >= 0 && gy < hf && F.mask[gy * wf + gx];
-            st[j] = !sys ? 0.0f : (m > 1e-30f ? st[j] / m : 1.0f);
+            st[j] = !sm[j] ? 0.0f : (m > 1e-30f ? st[j] / m : 1.0f);  // outside the level: mask 0
         }
     }
     __syncthreads();
@@ -153,8 +155,7 @@ __global__ void __launch_bounds__(CO_NT) mg_coarsen_kernel(MgLevel F, MgLevel C)
         for (int b = 0; b < 2; b++)
             for (int a = 0; a < 2; a++) {
                 const int q = (ly0 + b) * CO_R + lx0 + a;
-                const int gx = X0 + lx0 + a, gy = Y0 + ly0 + b;
-                if (gx >= wf || gy >= hf || !F.mask[gy * wf + gx]) continue;
+                if (!sm[q]) continue;
                 any = true;
                 const double tj = st[q];
                 const double at = (double)sc[q] * tj + (double)sdx[q - 1] * (tj - st[q - 1]) +
@@ -410,15 +411,19 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
         aug[n * m + k] = v;
     }
     __syncthreads();
-    const int na = n + 1;
+    // threads as 64 rows x 16 column lanes: thread (i, c) updates row i's active columns p + c, p + c + 16, ...
+    // (n <= 64 rows; n + 1 <= 65 active columns), no index divisions in the loop
+    const int i = threadIdx.x >> 4, c = threadIdx.x & 15;
     for (int p = 0; p < n; p++) {
         const double* src = aug + (p & 1) * n * m;
         double* dst = aug + ((p + 1) & 1) * n * m;
-        const double rpiv = 1.0 / src[p * m + p];
-        for (int k = threadIdx.x; k < n * na; k += blockDim.x) {
-            const int i = k / na, j = p + k % na;
-            const double apj = src[p * m + j] * rpiv;
-            dst[i * m + j] = i == p ? apj : src[i * m + j] - src[i * m + p] * apj;
+        if (i < n) {
+            const double rpiv = 1.0 / src[p * m + p];
+            const double aip = src[i * m + p];
+            for (int j = p + c; j <= n + p; j += 16) {
+                const double apj = src[p * m + j] * rpiv;
+                dst[i * m + j] = i == p ? apj : src[i * m + j] - aip * apj;
+            }
         }
         __syncthreads();
     }
