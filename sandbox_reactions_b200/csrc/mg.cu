@@ -412,17 +412,23 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
     }
     __syncthreads();
     // threads as 64 rows x 16 column lanes: thread (i, c) updates row i's active columns p + c, p + c + 16, ...
-    // (n <= 64 rows; n + 1 <= 65 active columns), no index divisions in the loop
+    // (n <= 64 rows; n + 1 <= 65 active columns), no index divisions in the loop; the thread that writes the next
+    // step's pivot also leaves its reciprocal for every thread to read
+    __shared__ double rpiv[2];
+    if (threadIdx.x == 0) rpiv[0] = 1.0 / aug[0];
+    __syncthreads();
     const int i = threadIdx.x >> 4, c = threadIdx.x & 15;
     for (int p = 0; p < n; p++) {
         const double* src = aug + (p & 1) * n * m;
         double* dst = aug + ((p + 1) & 1) * n * m;
         if (i < n) {
-            const double rpiv = 1.0 / src[p * m + p];
+            const double rp = rpiv[p & 1];
             const double aip = src[i * m + p];
             for (int j = p + c; j <= n + p; j += 16) {
-                const double apj = src[p * m + j] * rpiv;
-                dst[i * m + j] = i == p ? apj : src[i * m + j] - aip * apj;
+                const double apj = src[p * m + j] * rp;
+                const double v = i == p ? apj : src[i * m + j] - aip * apj;
+                dst[i * m + j] = v;
+                if (i == p + 1 && j == p + 1) rpiv[(p + 1) & 1] = 1.0 / v;
             }
         }
         __syncthreads();
