@@ -36,6 +36,7 @@ struct HydroConst {
     int w, h;
     int edge, limiter, bracket;
     float gamma, gm1, eps_floor, sigma_vac, sigma_floor;
+    float inv_gm1;  // 1 / (γ - 1)
 };
 
 struct Prim {
@@ -59,19 +60,19 @@ SR_HOST_DEVICE Prim eos_read(const HydroConst& H, float s, float mx, float my, f
         p.p = eos_pi(H, H.sigma_floor, H.eps_floor);
         return p;
     }
-    float kinetic = 0.5f * (mx * mx + my * my) / (s * s);
-    float raw = E / s - kinetic;
+    const float rs = 1.0f / s;  // one division per cell: the velocities and ε by products
+    p.u = mx * rs;
+    p.v = my * rs;
+    float raw = E * rs - 0.5f * (p.u * p.u + p.v * p.v);
     float eps = raw < H.eps_floor ? H.eps_floor : raw;
     p.s = s;
-    p.u = mx / s;
-    p.v = my / s;
     p.p = eos_pi(H, s, eps);
     return p;
 }
 
 // The conserved vector of primitives (hydro.rs:443-460).
 SR_HOST_DEVICE void eos_cons(const HydroConst& H, const Prim& p, float* U) {
-    float thermal = p.p / p.s / H.gm1;
+    float thermal = p.p / p.s * H.inv_gm1;
     float eps = fmaxf(thermal, H.eps_floor);
     U[0] = p.s;
     U[1] = p.s * p.u;
@@ -84,12 +85,14 @@ SR_HOST_DEVICE bool eos_prim(const HydroConst& H, const float* U, Prim& out) {
     float s = U[0];
     if (!(s > 0.0f)) return false;  // NaN or <= 0
     if (!(isfinite(U[0]) && isfinite(U[1]) && isfinite(U[2]) && isfinite(U[3]))) return false;
-    float raw = U[3] / s - 0.5f * (U[1] * U[1] + U[2] * U[2]) / (s * s);
+    const float rs = 1.0f / s;  // one division per state: the velocities and ε by products
+    const float u = U[1] * rs, v = U[2] * rs;
+    float raw = U[3] * rs - 0.5f * (u * u + v * v);
     if (!(raw > 0.0f)) return false;
     float eps = fmaxf(raw, H.eps_floor);
     out.s = s;
-    out.u = U[1] / s;
-    out.v = U[2] / s;
+    out.u = u;
+    out.v = v;
     out.p = eos_pi(H, s, eps);
     return true;
 }

@@ -90,6 +90,7 @@ static HydroConst hydro_const(const sr_config& c) {
     H.bracket = (int)c.thermal_bracket;
     H.gamma = (float)c.gamma;
     H.gm1 = (float)(c.gamma - 1.0);
+    H.inv_gm1 = (float)(1.0 / (c.gamma - 1.0));
     H.eps_floor = (float)(c.t_floor / c.mu / (c.gamma - 1.0));
     H.sigma_vac = (float)c.sigma_vac;
     H.sigma_floor = (float)c.sigma_floor;

@@ -34,14 +34,15 @@ __device__ __forceinline__ float lim(int which, float l, float c, float r) {
 
 // Limited slopes of (Σ, u, v, Π) along one axis; Σ and Π flat where the thermal bracket refuses a face
 // (hydro.rs:293-331, HOT_FACE = 2).
-__device__ __forceinline__ Prim slope(const HydroConst& H, const Prim& l, const Prim& c, const Prim& r) {
+__device__ __forceinline__ Prim slope(const HydroConst& H, const Prim& l, const Prim& c, const Prim& r, float ql,
+                                      float qc, float qr) {
     Prim s;
     s.s = lim(H.limiter, l.s, c.s, r.s);
     s.u = lim(H.limiter, l.u, c.u, r.u);
     s.v = lim(H.limiter, l.v, c.v, r.v);
     s.p = lim(H.limiter, l.p, c.p, r.p);
     if (H.bracket) {
-        float hottest = fmaxf(fmaxf(l.p / l.s, c.p / c.s), r.p / r.s);
+        float hottest = fmaxf(fmaxf(ql, qc), qr);  // Π/Σ of the three cells, staged once per cell
         float plo = c.p - 0.5f * s.p, blo = 2.0f * hottest * (c.s - 0.5f * s.s);
         float phi = c.p + 0.5f * s.p, bhi = 2.0f * hottest * (c.s + 0.5f * s.s);
         if (!(plo <= blo) || !(phi <= bhi)) {
@@ -77,10 +78,11 @@ __device__ __forceinline__ void evolved(const HydroConst& H, const Prim& base, c
 // The four predicted faces [x-, x+, y-, y+] of a cell and its centre's (Σ, Σu, Σv) half a step on (hydro.rs:587-614).
 // `want` is a bit mask of the faces the caller keeps.
 __device__ __forceinline__ void predict(const HydroConst& H, const Prim& l, const Prim& c, const Prim& r,
-                                        const Prim& up, const Prim& dn, float half, bool grav, float gx, float gy,
-                                        int want, Face* out, float* mid) {
-    Prim sx = slope(H, l, c, r);
-    Prim sy = slope(H, up, c, dn);
+                                        const Prim& up, const Prim& dn, const float* q, float half, bool grav,
+                                        float gx, float gy, int want, Face* out, float* mid) {
+    // q: Π/Σ of l, c, r, up, dn
+    Prim sx = slope(H, l, c, r, q[0], q[1], q[2]);
+    Prim sy = slope(H, up, c, dn, q[3], q[1], q[4]);
     Prim wf[4] = {offset(c, sx, -0.5f), offset(c, sx, 0.5f), offset(c, sy, -0.5f), offset(c, sy, 0.5f)};
     float uf[4][4];
 #pragma unroll
@@ -168,6 +170,7 @@ __device__ __forceinline__ void face_work(float q, float sl, float sh, float pl,
 struct __align__(16) Shared {
     float4 P[EY][EX];         // primitives (Σ, u, v, Π) of the staged region, ghosts included
     float S[EY][EX];          // raw Σ of the staged region (out-of-world: -1, read as vacuum)
+    float Q[EY][EX];          // Π/Σ of the staged region (the thermal bracket's temperatures)
     Face F[4][TY][TX];        // the tile's predicted faces
     Face FL[TY], FR[TY];      // x+ faces of the column left of the tile, x- faces of the column right of it
     Face FT[TX], FB[TX];      // y+ faces of the row above, y- faces of the row below
@@ -239,6 +242,7 @@ __global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 
         }
         sh.P[ly][lx] = make_float4(p.s, p.u, p.v, p.p);
         sh.S[ly][lx] = raw;
+        sh.Q[ly][lx] = p.p / p.s;
     }
     __syncthreads();
 
@@ -266,8 +270,9 @@ __global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 
         }
         Face f[4];
         float mid[3];
+        const float q[5] = {sh.Q[sy][sx - 1], sh.Q[sy][sx], sh.Q[sy][sx + 1], sh.Q[sy - 1][sx], sh.Q[sy + 1][sx]};
         predict(H, P_at(sh, sy, sx - 1), P_at(sh, sy, sx), P_at(sh, sy, sx + 1), P_at(sh, sy - 1, sx),
-                P_at(sh, sy + 1, sx), half, grav, gxv, gyv, want, f, mid);
+                P_at(sh, sy + 1, sx), q, half, grav, gxv, gyv, want, f, mid);
         if (k < NT) {
 #pragma unroll
             for (int q = 0; q < 4; q++) sh.F[q][ly][lx] = f[q];
