@@ -88,9 +88,10 @@ typedef struct sr_config {
     double kappa0;            /* opacity when no plane is given */
     double k_cond;            /* conduction coefficient */
     double chi;               /* > 0: the constant-diffusivity test flag (u = T, D_f = χ C_f) */
-    double solve_tol;         /* FP64 relative residual each Newton pass's linear solve reaches (1e-8) */
-    double newton_heat;       /* Newton stop: Σ C|ΔT| <= newton_heat Σ C T⁰ ... */
-    double newton_cell;       /* ... and every |ΔT| <= newton_cell T */
+    double solve_tol;         /* FP64 relative residual the last Newton pass's solve reaches (1e-8); earlier passes
+                                 are solved only as far as the Newton iteration needs */
+    double newton_heat;       /* Newton stop: Σ C|ΔT| <= newton_heat Σ C T⁰ (1e-6) ... */
+    double newton_cell;       /* ... and every |ΔT| <= newton_cell T (1e-3): the reference GPU path's rule */
     double dt_fixed;          /* > 0: every step runs on this Δt instead of the CFL/gravity one */
     double dt_cap;            /* > 0: Δt_{n+1} = min(Δt_{n+1}, dt_cap) (reference/mod.rs:213-216) */
     double mg_omega;          /* weight of the multigrid's coarse correction (0: the library's default) */

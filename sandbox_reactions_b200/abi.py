@@ -90,8 +90,8 @@ class Config:
     k_cond: float = 0.0
     chi: float = 0.0
     solve_tol: float = 1e-8
-    newton_heat: float = 1e-9
-    newton_cell: float = 1e-6
+    newton_heat: float = 1e-6   # the reference GPU path's Newton stop (crates/sr-engine/shaders/heat.wgsl:355-357)
+    newton_cell: float = 1e-3
     dt_fixed: float = 0.0
     dt_cap: float = 0.0
     mg_omega: float = 0.0

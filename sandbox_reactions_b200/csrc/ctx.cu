@@ -295,8 +295,8 @@ void sr_config_default(sr_config* c) {
     c->k_cond = 0.0;
     c->chi = 0.0;
     c->solve_tol = 1e-8;
-    c->newton_heat = 1e-9;
-    c->newton_cell = 1e-6;
+    c->newton_heat = 1e-6;  // the reference GPU path's Newton stop (crates/sr-engine/shaders/heat.wgsl:355-357)
+    c->newton_cell = 1e-3;
 }
 
 uint32_t sr_abi_version(void) { return SR_ABI_VERSION; }

@@ -1230,6 +1230,8 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     // new iterate anyway, and the last pass meets the same tolerances.
     const double tol = H->cfg.solve_tol;
     double pass_tol = std::max(tol, kFirstPassTol);
+    const double nheat = H->cfg.newton_heat, ncell = H->cfg.newton_cell;
+    double moved_prev = 0.0;
     build_system(H, dt, s);
     while (passes < H->max_passes && rounds < H->max_rounds) {
         passes++;
@@ -1239,17 +1241,22 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         R.rel_residual = S.rel;
         if (S.fallback) R.fallback_used = 1;
         if (!S.ok) break;
-        newton_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->cfg.newton_cell, dt, H->gas, H->C, H->t0,
+        newton_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, ncell, dt, H->gas, H->C, H->t0,
                                                               H->kvac, H->t, H->u, H->x, H->c64, H->rhs,
                                                               H->mg.L[0].c, H->red(S_MOVED));
         sr_note_launch();
         H->read(S_MOVED, 4, s);  // moved, violations, and the next system's two bounds
         const double rel_moved = heat0 > 0.0 ? H->hscal[S_MOVED] / heat0 : 0.0;
-        if (rel_moved <= H->cfg.newton_heat && H->hscal[S_VIOL] == 0.0 && pass_tol <= tol) {
+        if (rel_moved <= nheat && H->hscal[S_VIOL] == 0.0 && pass_tol <= tol) {
             converged = true;
             break;
         }
+        // the next pass is solved to solve_tol once it is expected to move less than newton_heat (the passes' observed
+        // contraction times this pass's move), since only a pass solved to solve_tol can end them
+        const double ratio = moved_prev > 0.0 ? std::min(1.0, std::max(0.01, rel_moved / moved_prev)) : 0.1;
+        moved_prev = rel_moved;
         pass_tol = std::max(tol, std::min(kFirstPassTol, rel_moved));
+        if (ratio * rel_moved <= nheat) pass_tol = tol;
         H->mg.coarsen(s);  // the next pass's coarse levels (its level-0 c is in place)
     }
     R.passes = passes;
