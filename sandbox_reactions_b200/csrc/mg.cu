@@ -1,4 +1,7 @@
 // mg.cu — the multigrid V-cycle (FP32) of the implicit FLD solve; see mg.cuh for the scheme.
+#include <algorithm>
+#include <map>
+#include <mutex>
 #include <utility>
 #include <vector>
 
@@ -813,6 +816,57 @@ void Multigrid::set_couplings(const double* kx, const double* ky, const uint8_t*
     sr_note_launch();
 }
 
+// The smoother tile of each level below 0 (level 0 keeps the CTA-count rule, which bounds its grid-sum partials),
+// chosen by timing on the level's first operator: per candidate (the big and the small tile) one warm-up pre- and
+// post-smoother, then the median of kTuneReps timed pairs; the rule's tile is kept unless the other is at least
+// kTuneMargin faster, so that run-to-run noise does not flip a choice. Choices are kept per level size for the process
+// (a batch's worlds of one size tune once).
+constexpr int kTuneReps = 7;
+constexpr float kTuneMargin = 0.95f;
+
+void Multigrid::autotune(cudaStream_t s) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int>, int> chosen;
+    tuned = true;
+    cudaEvent_t a, b;
+    SR_CUDA_TRY(cudaEventCreate(&a));
+    SR_CUDA_TRY(cudaEventCreate(&b));
+    for (int l = 1; l < tail; l++) {
+        const std::pair<int, int> key(L[l].w, L[l].h);
+        {
+            std::lock_guard<std::mutex> g(mu);
+            auto it = chosen.find(key);
+            if (it != chosen.end()) {
+                tile[l] = it->second;
+                continue;
+            }
+        }
+        float med[2];
+        for (int cand = 0; cand < 2; cand++) {
+            float t[kTuneReps];
+            for (int rep = -1; rep < kTuneReps; rep++) {  // rep -1 warms up
+                SR_CUDA_TRY(cudaEventRecord(a, s));
+                smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s, cand);
+                smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, nullptr, nullptr, nullptr, s, cand);
+                SR_CUDA_TRY(cudaEventRecord(b, s));
+                SR_CUDA_TRY(cudaEventSynchronize(b));
+                float ms = 0.0f;
+                SR_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+                if (rep >= 0) t[rep] = ms;
+            }
+            std::sort(t, t + kTuneReps);
+            med[cand] = t[kTuneReps / 2];
+        }
+        const int rule = small_tiles(L[l]) ? 1 : 0, other = 1 - rule;
+        const int pick = med[other] < kTuneMargin * med[rule] ? other : rule;
+        tile[l] = pick;
+        std::lock_guard<std::mutex> g(mu);
+        chosen[key] = pick;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+}
+
 void Multigrid::coarsen(cudaStream_t s) {
     for (int l = 1; l < nlevels; l++) {
         if (l == 1) {
@@ -827,13 +881,14 @@ void Multigrid::coarsen(cudaStream_t s) {
     const size_t nc = (size_t)C.w * C.h;
     mg_coarse_inverse_kernel<<<1, 1024, 2 * nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
     sr_note_launch();
+    if (!tuned) autotune(s);
 }
 
 void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter, double* rz_out, cudaStream_t s) {
     L[0].b = const_cast<float*>(r);
     L[0].x2 = z;
     for (int l = 0; l < tail; l++)
-        smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s);
+        smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s, tile[l]);
     TailArgs T;
     T.coarse_inv = coarse_inv;
     T.t = tail;
@@ -847,7 +902,7 @@ void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter,
     sr_note_launch();
     for (int l = tail - 1; l >= 0; l--)
         smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, l == 0 ? part : nullptr, l == 0 ? counter : nullptr,
-               l == 0 ? rz_out : nullptr, s);
+               l == 0 ? rz_out : nullptr, s, tile[l]);
 }
 
 void Multigrid::time_level0(int reps, void* flush, size_t flush_bytes, cudaStream_t s, double* pre_ms,

@@ -52,6 +52,10 @@ struct Multigrid {
     void coarsen(cudaStream_t s);
     // z = M r (level-0 b := r, x2 := z), and <r, z> into *rz_out (a one-launch grid sum over `part` and `counter`).
     void apply(const float* r, float* z, double* part, unsigned* counter, double* rz_out, cudaStream_t s);
+    // Picks each level's smoother tile by timing (after the first coarsening, outside any stream capture).
+    void autotune(cudaStream_t s);
+    int tile[kMgMaxLevels] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+    bool tuned = false;
     // The device time (ms) of one launch of level 0's pre- and post-smoother on the last applied system, each
     // averaged over `reps` launches with `flush` (flush_bytes, larger than L2) rewritten before each: a timing hook.
     void time_level0(int reps, void* flush, size_t flush_bytes, cudaStream_t s, double* pre_ms, double* post_ms);

@@ -1,5 +1,5 @@
 """Edge cases of the GPU path: a ragged, non-square world with vacuum holes (tile edges, odd coarse levels, masked
-cells, the small smoother tiles, the scalar-load fallbacks), and the largest world the ABI accepts (4096²,
+cells, the autotuner's small smoother tiles, the scalar-load fallbacks), and the largest world the ABI accepts (4096²,
 gravity padded to 8192²), checked through size-independent properties.
 
 Tolerances: the first system's solution within 1e-6 (max norm, relative) of a direct f64 solve, every implicit solve
