@@ -114,8 +114,9 @@ def committed_traffic(kernel: str, cells: int):
     return k["dram_bytes_per_launch"] * cells / k["cells"]
 
 
-def cpu_twin_sample(size: int, steps: int, threads: int):
-    """The oracle's f64 twin on a `size`² world of the benchmark's scene: (Mcell-steps/s, seconds, steps)."""
+def cpu_twin_sample(size: int, steps: int, threads: int, warmup: int = 0):
+    """The oracle's f64 twin on a `size`² world of the benchmark's scene, `warmup` untimed steps first:
+    (Mcell-steps/s, seconds, steps)."""
     import numpy as np
 
     import oracle as O
@@ -124,6 +125,7 @@ def cpu_twin_sample(size: int, steps: int, threads: int):
     O.set_threads(threads)
     cfg, P, kappa = scenes.full_step(size)
     twin = O.Twin(cfg, P.astype(np.float64), kappa.astype(np.float64))
+    twin.step(warmup)
     t0 = time.perf_counter()
     done = 0
     for _ in range(steps):
@@ -139,11 +141,11 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    value, secs, done = cpu_twin_sample(args.cpu_size, max(1, args.steps), threads)
+    value, secs, done = cpu_twin_sample(args.cpu_size, max(1, args.steps), threads, warmup=args.warmup)
     sample = (f"{done} twin steps of a {args.cpu_size}x{args.cpu_size} world of the benchmark scene "
               f"(hydro + gravity + FLD, f64, the reference's Jacobi-PCG to 1e-12), {secs:.1f} s on {threads} threads")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,
-            "warmup": 0, "ms_per_step": 1e3 * secs / max(done, 1), "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(done, 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"full step hydro+gravity+FLD, disk + opacity field + hot spots, "
                                    f"sample {args.cpu_size}x{args.cpu_size} of the {args.size}x{args.size} case",
