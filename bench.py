@@ -9,8 +9,16 @@ Under torchrun every rank advances its own world (scene seed = rank): the worlds
 data path, weak scaling. The line also carries the FLD time-to-1e-8 of the 2048² implicit-diffusion configuration
 (scenes.fld) with plain MG-PCG and with Jacobi-PCG.
 
-`--impl reference` times the reference's own CPU algorithm (the f64 twin restated in C, oracle/) on a bounded sample
-of the same workload with every host thread.
+`--impl reference` times the reference's own CPU algorithm (the f64 twin restated in C, oracle/) on the same 2048²
+world with every host thread, for as many of the K steps as fit a bounded time (at least one), and beside it one
+thread on a 512² sample of the scene.
+
+`--case fld|full|learned|sod|grav --size S` runs one small self-contained workload per hot kernel family instead (what
+the committed ncu summaries were captured on) and prints one line with its device time: fld, the implicit-diffusion
+world's first system solved to 1e-8 `--solves` times (smoothers, coarse tail, SpMV, PCG vectors); full, `--steps` full
+steps of the benchmark world; learned, one flexible-CG round with an untrained learned preconditioner (the convolution
+kernels' cost does not depend on the weights); sod, `--steps` hydro-only steps of a Sod tube (the stencil kernel);
+grav, `--solves` gravity-only steps of a disk (the FFT kernels).
 """
 from __future__ import annotations
 
@@ -114,45 +122,140 @@ def committed_traffic(kernel: str, cells: int):
     return k["dram_bytes_per_launch"] * cells / k["cells"]
 
 
-def cpu_twin_sample(size: int, steps: int, threads: int, warmup: int = 0):
-    """The oracle's f64 twin on a `size`² world of the benchmark's scene, `warmup` untimed steps first:
-    (Mcell-steps/s, seconds, steps)."""
+def cpu_twin_run(size: int, steps: int, threads: int, warmup: int = 0, budget_s: float = 20.0, world=None):
+    """The oracle's f64 twin (the reference's Twin, restated) on the `size`² world of the benchmark's scene: Twin::new
+    (P2 and Δt_0) and `warmup` steps untimed, then up to `steps` timed steps, stopping once `budget_s` seconds are spent
+    (at least one). Returns (Mcell-steps/s, seconds, steps timed, twin)."""
     import numpy as np
 
     import oracle as O
     from sandbox_reactions_b200 import scenes
 
     O.set_threads(threads)
-    cfg, P, kappa = scenes.full_step(size)
+    cfg, P, kappa = world if world is not None else scenes.full_step(size)
     twin = O.Twin(cfg, P.astype(np.float64), kappa.astype(np.float64))
     twin.step(warmup)
     t0 = time.perf_counter()
     done = 0
-    for _ in range(steps):
+    for _ in range(max(1, steps)):
         twin.step(1)
         done += 1
-        if time.perf_counter() - t0 > 20.0:
+        if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return size * size * done / dt / 1e6, dt, done
+    return size * size * done / dt / 1e6, dt, done, twin
+
+
+def workload_config(n: int, world: int) -> dict:
+    return {"workload": f"full step hydro+gravity+FLD, {n}x{n}, Gaussian disk + lognormal opacity "
+                        f"(32-cell correlation, 6 decades) + hot spots; FFT {2 * n}x{2 * n}",
+            "cells": n * n, "parallelism": f"replicas x{world}",
+            "l2": "working set larger than L2 (state, fields and solver planes > 1 GB)"}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the twin on the benchmark's own world (same scene, size and seed as this arm's rank 0),
+    every host thread; W is capped at one untimed step (the CPU has nothing to warm beyond its caches) and the timed
+    steps stop at K or once --ref-budget seconds are spent. One thread on a 512² sample rides along."""
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    value, secs, done = cpu_twin_sample(args.cpu_size, max(1, args.steps), threads, warmup=args.warmup)
-    sample = (f"{done} twin steps of a {args.cpu_size}x{args.cpu_size} world of the benchmark scene "
-              f"(hydro + gravity + FLD, f64, the reference's Jacobi-PCG to 1e-12), {secs:.1f} s on {threads} threads")
+    n = args.size
+    warm = min(args.warmup, 1)
+    value, secs, done, _ = cpu_twin_run(n, args.steps, threads, warmup=warm, budget_s=args.ref_budget)
+    sample = (f"{done} twin steps of the {n}x{n} benchmark world itself (hydro + gravity + FLD, f64, the reference's "
+              f"Jacobi-PCG to 1e-12), {secs:.1f} s on {threads} threads after Twin::new and {warm} untimed step(s)")
+    one_n = min(512, n)
+    v1, s1, d1, _ = cpu_twin_run(one_n, 1, 1, budget_s=0.0)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": done,
-            "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(done, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"full step hydro+gravity+FLD, disk + opacity field + hot spots, "
-                                   f"sample {args.cpu_size}x{args.cpu_size} of the {args.size}x{args.size} case",
-                       "cells": args.cpu_size ** 2, "parallelism": "host threads"},
+            "warmup": args.warmup, "warmup_steps_run": warm, "steps_requested": args.steps,
+            "ms_per_step": 1e3 * secs / max(done, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(n, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "one_thread": {"value": v1, "unit": UNIT, "cores": 1, "kind": "port",
+                           "sample": f"{d1} twin step of a {one_n}x{one_n} world of the same scene, {s1:.1f} s"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def rel_l1(a, b) -> float:
+    import numpy as np
+
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
+
+
+def full_step_parity(step, twin, P, kappa) -> dict:
+    """One GPU step of the benchmark world from the same f32 start as the twin's step: rel L1 per field (the bar is
+    1e-5) and the implicit solve's FP64 residual (the bar is 1e-8)."""
+    step.upload(P)
+    step.upload_opacity(kappa)
+    step.run(1)
+    gpu = step.readback()
+    heat = step.read_heat()
+    ref = twin.state()
+    errs = {name: rel_l1(gpu[k], ref[k]) for k, name in enumerate(("sigma", "sigma_u", "sigma_v", "E"))}
+    return {"what": "one step from the same f32 start vs the f64 twin (Newton 1e-12, Jacobi-PCG 1e-12)",
+            "rel_l1": errs, "max_rel_l1": max(errs.values()), "bar": 1e-5, "heat_rel_residual": heat.rel_residual,
+            "heat_passes": heat.passes, "ok": max(errs.values()) <= 1e-5 and heat.rel_residual <= 1e-8}
+
+
+def run_case(args, local):
+    """One profiling workload (see the module docstring); prints one line with its device time."""
+    import torch
+
+    from sandbox_reactions_b200 import build as lib_build
+    from sandbox_reactions_b200 import scenes
+    from sandbox_reactions_b200.engine import Learner, Step
+
+    torch.cuda.set_device(local)
+    lib_build.build()
+    n = args.size
+    if args.case == "fld":
+        cfg, P, kappa = scenes.fld(n)
+        with Step(cfg) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            for _ in range(args.solves):
+                ms, rounds, rel, _ = s.heat_first_solve(cfg.dt_fixed, args.precond)
+        print(f"fld {n}: {args.precond} first solve {ms:.3f} ms, {rounds} rounds, rel residual {rel:.2e}")
+    elif args.case == "full":
+        cfg, P, kappa = scenes.full_step(n)
+        with Step(cfg) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            s.set_timing(True)
+            s.run(args.steps)
+            cost = s.read_cost()
+        print(f"full {n}: {args.steps} steps, {cost.total_ms / args.steps:.3f} ms per step")
+    elif args.case == "learned":
+        cfg, P, kappa = scenes.fld(n)
+        with Learner(crop=64, capacity=1, seed=1) as L, Step(cfg) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            s.attach_learner(L)
+            s.set_heat_limits(128, 1)
+            ms, _, _, _ = s.heat_first_solve(cfg.dt_fixed, "learned")
+            s.attach_learner(None)
+        print(f"learned {n}: one round {ms:.3f} ms")
+    elif args.case == "sod":
+        cfg, P = scenes.sod(n)
+        with Step(cfg) as s:
+            s.upload(P)
+            s.set_timing(True)
+            s.run(args.steps)
+            cost = s.read_cost()
+        print(f"sod {n}: {args.steps} steps, {cost.total_ms / args.steps:.3f} ms per step")
+    else:
+        cfg, P = scenes.disk(n)
+        with Step(cfg.replace(hydro=False, heat=False)) as s:
+            s.upload(P)
+            s.set_timing(True)
+            s.run(args.solves)  # each step: P2's solve, P8, P9
+            cost = s.read_cost()
+        print(f"grav {n}: {args.solves} solves, {cost.gravity_ms / args.solves:.3f} ms per solve")
     return 0
 
 
@@ -195,10 +298,13 @@ def fld_time_to_tol(size: int):
         s.upload_opacity(kappa)
         if learner is not None:
             s.attach_learner(learner)
+        x_mg = None
         for pc in ("mg", "jacobi", "learned"):
             try:
                 s.heat_first_solve(cfg.dt_fixed, pc)  # warm-up
-                ms, rounds, rel, _ = s.heat_first_solve(cfg.dt_fixed, pc)
+                ms, rounds, rel, x = s.heat_first_solve(cfg.dt_fixed, pc, want_x=(pc == "mg"))
+                if pc == "mg":
+                    x_mg = x
                 out[pc] = {"ms": ms, "rounds": rounds, "rel_residual": rel}
                 if pc == "learned":
                     out[pc]["fallback"] = s.last_fallback
@@ -209,32 +315,102 @@ def fld_time_to_tol(size: int):
         learner.close()
     if "ms" in out.get("learned", {}) and "ms" in out.get("mg", {}):
         out["learned_speedup_vs_mg"] = out["mg"]["ms"] / out["learned"]["ms"]
+    out.update(fld_system_checks(cfg, P, kappa, x_mg))
+    return out
+
+
+def system_stiffness(diag, kx, ky, gas) -> dict:
+    """How far the implicit system is from its diagonal: per cell, the couplings' sum Σ_f D_f Δt over the mass term
+    C/(4 a_r T³) (= the cell's Δt over its explicit diffusion limit)."""
+    import numpy as np
+
+    off = np.zeros_like(diag)
+    off[:, :] += kx[:, :-1] + kx[:, 1:]
+    off[:, :] += ky[:-1, :] + ky[1:, :]
+    mass = diag - off
+    r = (off / np.maximum(mass, 1e-300))[gas.astype(bool)]
+    return {"max": float(r.max()), "median": float(np.median(r)), "p99": float(np.percentile(r, 99))}
+
+
+def fld_system_checks(cfg, P, kappa, x_mg) -> dict:
+    """The implicit-diffusion world's first system, built by the oracle: its stiffness, and the GPU's MG-PCG solution
+    against the twin's f64 Jacobi-PCG solve to 1e-12 (max norm over gas cells, relative; the bar is 1e-6)."""
+    import numpy as np
+
+    import oracle as O
+
+    O.set_threads(os.cpu_count() or 1)
+    diag, rhs, kx, ky, gas = O.heat_system(cfg, P.astype(np.float64), cfg.dt_fixed, kappa.astype(np.float64))
+    out = {"stiffness": system_stiffness(diag, kx, ky, gas)}
+    if x_mg is not None:
+        x_ref, rounds = O.heat_pcg(diag, rhs, kx, ky, gas, rel=1e-12, max_rounds=200000)
+        g = gas.astype(bool)
+        out["parity"] = {"solution_max_rel": float(np.abs(x_mg - x_ref)[g].max() / np.abs(x_ref[g]).max()),
+                         "bar": 1e-6, "twin_rounds_to_1e-12": rounds}
     return out
 
 
 def config_runs(peak_gbs: float):
     """The other single-GPU configurations as side measurements (device time of the steps, library events): C1, the
     Sod tube at 512² with minmod (hydro only, 200 steps), and C2, the disk at 1024² with its FFT gravity (100 steps);
-    each with its hydro update kernel's HBM roofline (32 B/cell without gravity, 56 B/cell with)."""
+    each with its hydro update kernel's HBM roofline (32 B/cell without gravity, 56 B/cell with) and its parity: one
+    GPU step against the oracle's step from the same f32 start (bar 1e-5 per field); for C1 also the 200 steps against
+    the twin's (the reference's G-REF band, 1e-3), for C2 the start state's potential against an f64 direct sum on a
+    128² subsample of target cells."""
+    import numpy as np
+
+    import oracle as O
     from sandbox_reactions_b200 import scenes
     from sandbox_reactions_b200.engine import Step
 
+    O.set_threads(os.cpu_count() or 1)
     out = {}
     for name, (cfg, P), steps, bpc in (("C1_sod_512_minmod", scenes.sod(512), 200, 32),
                                        ("C2_disk_hydro_grav_1024", scenes.disk(1024), 100, 56)):
         with Step(cfg) as s:
             s.upload(P)
-            s.run(3)
+            phi = s.gravity_field()[0] if cfg.gravity else None
+            s.run(1)
+            one = s.readback()
+            dt1 = s.read_dt().dt
+            s.run(2)
             s.set_timing(True)
             s.run(steps)
             c = s.read_cost()
+            s.set_timing(False)
+            if not cfg.gravity:
+                s.upload(P)
+                s.run(steps)
+                final = s.readback()
+                sim_time = s.read_dt().sim_time
         n = cfg.width * cfg.height
         upd = c.hydro_update_ms / max(1, c.hydro_update_launches)
         gbs = bpc * n / (upd / 1e3) / 1e9
+        P64 = P.astype(np.float64)
+        g = O.grav_field(cfg, P64[0])[1:] if cfg.gravity else None
+        ref = O.floors(cfg, O.hydro_step(cfg, P64, dt1, g)[0])
+        par = {"one_step_rel_l1": max(rel_l1(one[k], ref[k]) for k in range(4) if np.abs(ref[k]).sum() > 0),
+               "bar": 1e-5}
+        if not cfg.gravity:
+            twin = O.Twin(cfg, P64)
+            twin.step(steps)
+            tref = twin.state()
+            par[f"{steps}_steps_rel_l1"] = {"sigma": rel_l1(final[0], tref[0]), "E": rel_l1(final[3], tref[3]),
+                                           "clock": abs(sim_time - twin.clock()["sim_time"]) / twin.clock()["sim_time"],
+                                           "bar": 1e-3}
+        else:
+            src = np.where(P[0] >= np.float32(cfg.sigma_vac), P[0], 0.0).astype(np.float64)
+            ty, tx = np.mgrid[4:cfg.height:8, 4:cfg.width:8]
+            direct = O.direct_potential(cfg, src, tx.ravel(), ty.ravel())
+            got = phi[ty.ravel(), tx.ravel()]
+            par["potential_vs_direct_sum"] = {"rel_l1": rel_l1(got, direct),
+                                              "max_rel": float((np.abs(got - direct) / np.abs(direct)).max()),
+                                              "targets": int(direct.size)}
         out[name] = {"value": n * steps / (c.total_ms / 1e3) / 1e6, "unit": "Mcell-steps/s", "steps": steps,
                      "ms_per_step": c.total_ms / steps,
                      "hydro_update": {"ms_per_launch": upd, "algorithmic_bytes_per_cell": bpc, "achieved_gbs": gbs,
-                                      "frac_of_measured_hbm": gbs / peak_gbs}}
+                                      "frac_of_measured_hbm": gbs / peak_gbs},
+                     "parity": par}
     return out
 
 
@@ -307,8 +483,13 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--size", type=int, default=2048)
-    ap.add_argument("--cpu-size", type=int, default=256)
+    ap.add_argument("--ref-budget", type=float, default=120.0,
+                    help="seconds of timed twin steps the reference arm may spend (at least one step)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--case", choices=["fld", "full", "learned", "sod", "grav"],
+                    help="run one profiling workload instead of the benchmark")
+    ap.add_argument("--solves", type=int, default=3)
+    ap.add_argument("--precond", default="mg")
     ap.add_argument("--no-fld", action="store_true", help="skip the FLD time-to-1e-8 measurement")
     ap.add_argument("--batch", type=int, default=0,
                     help="run config 5 instead: this many worlds of a seeded 256..2048 mix, batched vs one at a time")
@@ -317,6 +498,8 @@ def main():
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.case:
+        return run_case(args, local)
     if args.batch:
         return run_batch(args, rank, world, local)
 
@@ -397,6 +580,17 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     e2e_value = world * n * n * e2e_steps / (float(t.item()) / 1e3) / 1e6
 
+    cpu = parity = None
+    if rank == 0 and world == 1:
+        # the CPU baseline on the same world: one f64 twin step of the benchmark's own start state, all host threads;
+        # its result doubles as the full-size parity check of one GPU step from the same f32 start
+        threads = os.cpu_count() or 1
+        v, secs, done, twin = cpu_twin_run(n, 1, threads, budget_s=0.0, world=(cfg, P, kappa))
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{done} f64 twin step of the {n}x{n} benchmark world itself (Twin::new untimed), "
+                         f"{secs:.1f} s on {threads} threads"}
+        parity = full_step_parity(step, twin, P, kappa)
+        del twin
     fld = None
     configs = None
     if rank == 0 and not args.no_fld and world == 1:
@@ -425,22 +619,12 @@ def main():
                         "achieved": upd_gbs, "frac": upd_gbs / peak, "ms_per_launch": upd_ms,
                         "algorithmic_bytes_per_cell": HYDRO_UPDATE_BYTES_PER_CELL,
                         "traffic": committed_traffic("hydro_update", n * n)}}}
-        cpu = None
-        if world == 1:
-            threads = os.cpu_count() or 1
-            v, secs, done = cpu_twin_sample(args.cpu_size, 50, threads)
-            cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                   "sample": f"{done} f64 twin steps of a {args.cpu_size}x{args.cpu_size} world of the same scene, "
-                             f"{secs:.1f} s"}
         clocks = sampler.summary()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"full step hydro+gravity+FLD, {n}x{n}, Gaussian disk + lognormal opacity "
-                                   f"(32-cell correlation, 6 decades) + hot spots; FFT {2 * n}x{2 * n}",
-                       "cells": n * n, "parallelism": f"replicas x{world}",
-                       "l2": "working set larger than L2 (state, fields and solver planes > 1 GB)"},
+            "config": workload_config(n, world),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 5 * 4 * n * n,
                     "d2h_bytes_per_step": 4 * 4 * n * n, "steps": e2e_steps},
             "gpu_launches": int(cost.kernel_launches),
@@ -451,6 +635,7 @@ def main():
                                       "heat": cost.heat_ms / args.steps, "floors_dt": cost.dt_ms / args.steps},
             "heat_last_step": {"passes": heat.passes, "rounds": heat.rounds, "refinements": heat.refinements,
                                "converged": heat.converged, "rel_residual": heat.rel_residual},
+            "parity": parity,
             "fld_time_to_1e-8": fld,
             "other_configs": configs,
         }

@@ -254,9 +254,10 @@ sr_ctx* sr_batch_ctx(sr_batch* b, uint32_t index);
  * caller passes device buffers: `sigma` (W*H) in, `phi`, `gx`, `gy` (W*H each) out, and the CUDA stream (NULL: the
  * default stream) as `stream`. The scratch lives in static device arrays sized for worlds up to 256 x 256 cells, held
  * by every GPU that loads the library until exit; a larger world is refused with SR_E_INVALID. The first call on a
- * device looks up the arrays and uploads the kernel's spectrum, so it should come before any stream capture. Calls
- * share the arrays: calls whose work overlaps on the GPU race. Uses cfg's width, height, kernel, G, softening and
- * sigma_vac. */
+ * device looks up the arrays and uploads the kernel's spectrum; so does every call whose padded FFT size, kernel, G or
+ * (softened kernel only) softening differs from the previous call's on that device. Such a call copies from the host
+ * and waits for `stream`, blocking the host: it must not be made during a stream capture. Calls share the arrays:
+ * calls whose work overlaps on the GPU race. Uses cfg's width, height, kernel, G, softening and sigma_vac. */
 sr_status sr_gravity_solve_static(const sr_config* cfg, const float* sigma, float* phi, float* gx, float* gy,
                                   void* stream);
 

@@ -10,11 +10,12 @@
 //
 // Host code never hands a static array's name to a kernel: a __device__ array's name is a host-side stand-in, not a
 // device address. Once per device, with that device current, the first call looks up each array's device address with
-// cudaGetSymbolAddress (checking every return code) and keeps them; that first call, and any call that changes the
-// padded size or the gravity kernel, also uploads the kernel's spectrum and twiddles (a synchronous copy), so the
-// first call on a device should come before any stream capture. Calls share the arrays: two calls whose work overlaps
-// on the GPU race. No buffer needs clearing between calls: every value a kernel reads was written earlier in the same
-// call.
+// cudaGetSymbolAddress (checking every return code) and keeps them. That first call, and every later call whose
+// padded size, gravity kernel, G or (for the softened kernel) softening differs from the previous call's on the same
+// device, also builds the kernel's spectrum and twiddles on the host, copies them up and waits for the caller's stream
+// (the host staging is reused), so such a call blocks the host and must not be made during a stream capture. Calls
+// share the arrays: two calls whose work overlaps on the GPU race. No buffer needs clearing between calls: every value
+// a kernel reads was written earlier in the same call.
 #include <math.h>
 #include <string.h>
 
@@ -129,6 +130,9 @@ void upload_tables(DeviceSlot& d, int px, int py, int kind, double G, double eps
         h_tw[kStaticMaxPadded + k] = make_float2((float)cos(a), (float)sin(a));
     }
     const size_t kq = (size_t)(px / 2 + 1) * (py / 2 + 1);
+    // forget what the arrays held before the copies start: if one of them fails, the next call uploads again
+    d.kind = -1;
+    d.px = d.py = 0;
     check(cudaMemcpyAsync(d.khat, h_khat, sizeof(float) * kq, cudaMemcpyHostToDevice, s), "copy K̂ to the static array");
     check(cudaMemcpyAsync(d.tw, h_tw, sizeof(float2) * 2 * kStaticMaxPadded, cudaMemcpyHostToDevice, s),
           "copy the twiddles to the static array");
@@ -172,8 +176,10 @@ extern "C" sr_status sr_gravity_solve_static(const sr_config* cfg, const float* 
             d.ready = true;
         }
         const int px = grav_padded_size(w), py = grav_padded_size(h);
-        if (d.px != px || d.py != py || d.kind != (int)cfg->kernel || d.G != cfg->G || d.eps != cfg->softening)
-            upload_tables(d, px, py, (int)cfg->kernel, cfg->G, cfg->softening, s);
+        // the self-cell kernel ignores the softening, so a change of it alone keeps the tables
+        const double eps = cfg->kernel == SR_KERNEL_SOFTENED ? cfg->softening : 0.0;
+        if (d.px != px || d.py != py || d.kind != (int)cfg->kernel || d.G != cfg->G || d.eps != eps)
+            upload_tables(d, px, py, (int)cfg->kernel, cfg->G, eps, s);
         // the allocating path's kernels, their scratch pointed at the static arrays
         GravPlan plan;
         plan.w = w;

@@ -48,6 +48,33 @@ def test_the_static_solve_matches_the_allocating_path_on_two_calls():
             o.fill_(float("nan"))
 
 
+def test_the_static_solve_rebuilds_its_tables_when_the_world_or_kernel_changes():
+    # 192x128 self-cell, 64x64 softened, 192x128 self-cell again on one device: every change of padded size and
+    # kernel rebuilds the spectrum in the static arrays; each call is held to a fresh context's P2.
+    import torch
+
+    lib = load_library()
+    base, P = scenes.disk(256)
+    cases = [(192, 128, "self_cell"), (64, 64, "softened"), (192, 128, "self_cell")]
+    stream = torch.cuda.current_stream()
+    for w, h, kernel in cases:
+        cfg = base.replace(width=w, height=h, hydro=False, kernel=kernel)
+        Q = np.ascontiguousarray(P[:, 128 - h // 2:128 + h // 2, 128 - w // 2:128 + w // 2])
+        with Step(cfg) as s:
+            s.upload(Q)
+            phi0, gx0, gy0 = s.gravity_field()
+        c = cfg.to_c()
+        sigma = torch.from_numpy(np.ascontiguousarray(Q[0])).cuda()
+        outs = [torch.full((h, w), float("nan"), device="cuda") for _ in range(3)]
+        st = lib.sr_gravity_solve_static(C.byref(c), sigma.data_ptr(), outs[0].data_ptr(), outs[1].data_ptr(),
+                                         outs[2].data_ptr(), C.c_void_p(stream.cuda_stream))
+        assert st == 0, lib.sr_last_error(None).decode()
+        torch.cuda.synchronize()
+        phi, gx, gy = (o.cpu().numpy() for o in outs)
+        assert rel_l1(phi, phi0) <= 1e-5, (w, h, kernel, rel_l1(phi, phi0))
+        assert rel_l1(gx, gx0) <= 1e-5 and rel_l1(gy, gy0) <= 1e-5, (w, h, kernel)
+
+
 def test_the_static_solve_refuses_a_world_past_its_scratch():
     import torch
 
