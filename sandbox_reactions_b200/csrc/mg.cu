@@ -385,6 +385,175 @@ __global__ void __launch_bounds__(NT) mg_smooth_kernel(MgLevel L, MgLevel C, con
     }
 }
 
+// The row-band smoother of the big levels of even width: the same smoother as mg_smooth_kernel (NS red-black
+// half-sweeps of a tile whose halo is as deep as the half-sweeps, then the restriction or <b, x2>), with every cell's
+// coefficients and iterate held in registers. A CTA covers a 64 x 64 region (RB_RX x RB_RY): warp w owns rows
+// 4w .. 4w+3 (a band), lane j owns the cell pair (2j, 2j+1) of each of its rows. In a half-sweep a cell's horizontal
+// neighbours are its pair partner (a register) and one cell of the next lane's pair (a shuffle), its vertical
+// neighbours the same lane's rows above and below (registers), except across a band edge, whose rows go through shared
+// memory once per half-sweep (double-buffered: one barrier per half-sweep). Which cell of a pair a colour updates is
+// fixed by the row's parity (the region starts on an even column and row, so local parity = global parity), so the
+// sweeps unroll into straight-line code. The halo is NS + 2 for the pre-smoother (NS + 1 keeps the restriction's
+// neighbours exact; one more keeps the region on even columns, so pairs load as 8-byte words and sit inside one 2 x 2
+// aggregate) and NS for the post-smoother. Cells outside the level: b = 0, c = 1, no couplings, inverse diagonal 0.
+constexpr int RB_R = 4, RB_WARPS = 16, RB_NT = 32 * RB_WARPS, RB_RX = 64, RB_RY = RB_R * RB_WARPS;
+
+template <int NS, bool PRE>
+constexpr int rb_halo() { return PRE ? NS + 2 : NS; }
+
+template <int NS, bool PRE, bool WT>
+__global__ void __launch_bounds__(RB_NT, 2) mg_rowband_kernel(MgLevel L, MgLevel C, const float* __restrict__ xc,
+                                                            float omega, double* part, unsigned* counter,
+                                                            double* out) {
+    constexpr int H = rb_halo<NS, PRE>(), SX = RB_RX - 2 * H, SY = RB_RY - 2 * H;
+    static_assert(H % 2 == 0 && NS % 2 == 0, "the region starts on an even column and row");
+    __shared__ float2 edge[2][2][RB_WARPS][32];  // [buffer][top row / bottom row][warp][lane]: (x of 2j, x of 2j+1)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int w = L.w, h = L.h;
+    const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * SY - H;
+    const int gx = X0 + 2 * lane;             // the pair's first column (even)
+    const bool xin = gx >= 0 && gx < w;        // w is even: both cells of the pair lie inside, or neither
+    const int gy0 = Y0 + RB_R * warp;          // the band's first row (even)
+
+    float bA[RB_R], bB[RB_R], iA[RB_R], iB[RB_R], dl[RB_R], dm[RB_R], dr[RB_R], dA[RB_R], dB[RB_R];
+    float xA[RB_R], xB[RB_R], cA[RB_R], cB[RB_R];
+    float uA = 0.0f, uB = 0.0f;  // the couplings of row 0 to the row above
+#pragma unroll
+    for (int r = 0; r < RB_R; r++) {
+        const int gy = gy0 + r;
+        const bool in = xin && gy >= 0 && gy < h;
+        const size_t i = (size_t)gy * w + gx;
+        float2 b2 = make_float2(0.f, 0.f), c2 = make_float2(1.f, 1.f), dx2 = b2, dy2 = b2;
+        if (in) {
+            b2 = *reinterpret_cast<const float2*>(L.b + i);
+            c2 = *reinterpret_cast<const float2*>(L.c + i);
+            dx2 = *reinterpret_cast<const float2*>(L.dx + i);
+            dy2 = *reinterpret_cast<const float2*>(L.dy + i);
+            if (r == 0 && gy > 0) {
+                const float2 u2 = *reinterpret_cast<const float2*>(L.dy + i - w);
+                uA = u2.x;
+                uB = u2.y;
+            }
+        }
+        bA[r] = b2.x;
+        bB[r] = b2.y;
+        cA[r] = c2.x;
+        cB[r] = c2.y;
+        dm[r] = dx2.x;
+        dr[r] = dx2.y;
+        dA[r] = dy2.x;
+        dB[r] = dy2.y;
+        // the coupling of cell 2j to 2j - 1 is the previous pair's right coupling (0 from a pair outside the level)
+        dl[r] = __shfl_up_sync(0xffffffffu, dx2.y, 1);
+        if (lane == 0) dl[r] = (in && gx > 0) ? L.dx[i - 1] : 0.0f;
+        const float upA = r ? dA[r - 1] : uA, upB = r ? dB[r - 1] : uB;
+        iA[r] = in ? __fdividef(1.0f, c2.x + dl[r] + dx2.x + upA + dy2.x) : 0.0f;
+        iB[r] = in ? __fdividef(1.0f, c2.y + dx2.x + dx2.y + upB + dy2.y) : 0.0f;
+        float x0 = 0.0f, x1 = 0.0f;
+        if (!PRE && in) {
+            const float2 xv = *reinterpret_cast<const float2*>(L.x + i);
+            const float corr = omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)];
+            if constexpr (WT) {
+                const float2 t2 = *reinterpret_cast<const float2*>(L.t + i);
+                x0 = xv.x + corr * t2.x;
+                x1 = xv.y + corr * t2.y;
+            } else {
+                x0 = xv.x + corr;
+                x1 = xv.y + corr;
+            }
+        }
+        xA[r] = x0;
+        xB[r] = x1;
+    }
+    edge[0][0][warp][lane] = make_float2(xA[0], xB[0]);
+    edge[0][1][warp][lane] = make_float2(xA[RB_R - 1], xB[RB_R - 1]);
+    __syncthreads();
+    const int wu = warp > 0 ? warp - 1 : warp, wd = warp + 1 < RB_WARPS ? warp + 1 : warp;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const int col = PRE ? (s & 1) : 1 - (s & 1);
+        const int rd = s & 1, wr = (s + 1) & 1;
+        const float2 above = edge[rd][1][wu][lane], below = edge[rd][0][wd][lane];
+#pragma unroll
+        for (int r = 0; r < RB_R; r++) {
+            if ((r & 1) == col) {  // the pair's first cell has this colour
+                const float left = __shfl_up_sync(0xffffffffu, xB[r], 1);
+                const float up = r ? xA[r - 1] : above.x, down = r + 1 < RB_R ? xA[r + 1] : below.x;
+                const float cu = r ? dA[r - 1] : uA;
+                xA[r] = (bA[r] + dl[r] * left + dm[r] * xB[r] + cu * up + dA[r] * down) * iA[r];
+            } else {
+                const float right = __shfl_down_sync(0xffffffffu, xA[r], 1);
+                const float up = r ? xB[r - 1] : above.y, down = r + 1 < RB_R ? xB[r + 1] : below.y;
+                const float cu = r ? dB[r - 1] : uB;
+                xB[r] = (bB[r] + dm[r] * xA[r] + dr[r] * right + cu * up + dB[r] * down) * iB[r];
+            }
+        }
+        edge[wr][0][warp][lane] = make_float2(xA[0], xB[0]);
+        edge[wr][1][warp][lane] = make_float2(xA[RB_R - 1], xB[RB_R - 1]);
+        __syncthreads();
+    }
+    const bool xout = xin && 2 * lane >= H && 2 * lane < RB_RX - H;
+    if constexpr (PRE) {
+        const float2 above = edge[NS & 1][1][wu][lane], below = edge[NS & 1][0][wd][lane];
+        float ragg[RB_R / 2] = {};
+#pragma unroll
+        for (int r = 0; r < RB_R; r++) {
+            const int gy = gy0 + r, ly = RB_R * warp + r;
+            const bool o = xout && ly >= H && ly < RB_RY - H && gy < h;
+            const size_t i = (size_t)gy * w + gx;
+            if (o) *reinterpret_cast<float2*>(L.x + i) = make_float2(xA[r], xB[r]);
+            // the residual in difference form, c x + Σ d (x - x_nb), for both cells
+            const float left = __shfl_up_sync(0xffffffffu, xB[r], 1);
+            const float right = __shfl_down_sync(0xffffffffu, xA[r], 1);
+            const float upA = r ? xA[r - 1] : above.x, dnA = r + 1 < RB_R ? xA[r + 1] : below.x;
+            const float upB = r ? xB[r - 1] : above.y, dnB = r + 1 < RB_R ? xB[r + 1] : below.y;
+            const float cuA = r ? dA[r - 1] : uA, cuB = r ? dB[r - 1] : uB;
+            float axA = cA[r] * xA[r];
+            axA += dl[r] * (xA[r] - left);
+            axA += dm[r] * (xA[r] - xB[r]);
+            axA += cuA * (xA[r] - upA);
+            axA += dA[r] * (xA[r] - dnA);
+            float axB = cB[r] * xB[r];
+            axB += dm[r] * (xB[r] - xA[r]);
+            axB += dr[r] * (xB[r] - right);
+            axB += cuB * (xB[r] - upB);
+            axB += dB[r] * (xB[r] - dnB);
+            float rA = bA[r] - axA, rB = bB[r] - axB;
+            if constexpr (WT) {
+                if (o) {
+                    const float2 t2 = *reinterpret_cast<const float2*>(L.t + i);
+                    rA *= t2.x;
+                    rB *= t2.y;
+                }
+            }
+            ragg[r >> 1] += rA + rB;
+        }
+#pragma unroll
+        for (int k = 0; k < RB_R / 2; k++) {
+            const int ly = RB_R * warp + 2 * k;
+            const int X = gx >> 1, Y = (gy0 + 2 * k) >> 1;
+            if (xout && ly >= H && ly < RB_RY - H && X < C.w && Y < C.h && gy0 + 2 * k >= 0) {
+                const size_t I = (size_t)Y * C.w + X;
+                C.b[I] = C.mask[I] ? ragg[k] : 0.0f;
+            }
+        }
+    } else {
+        double acc = 0.0;
+#pragma unroll
+        for (int r = 0; r < RB_R; r++) {
+            const int gy = gy0 + r, ly = RB_R * warp + r;
+            if (xout && ly >= H && ly < RB_RY - H && gy < h) {
+                const size_t i = (size_t)gy * w + gx;
+                *reinterpret_cast<float2*>(L.x2 + i) = make_float2(xA[r], xB[r]);
+                if (out) acc += (double)bA[r] * (double)xA[r] + (double)bB[r] * (double)xB[r];
+            }
+        }
+        if (out) grid_sum_last1(acc, part, counter, out);
+    }
+    (void)SX;
+    (void)SY;
+}
+
 // The coarsest level's operator inverted by Gauss-Jordan elimination in f64 in one CTA (n <= 64 cells), masked-out
 // cells as identity rows; stored f32. The operator is SPD, so no pivoting is needed. The augmented matrix [A | I] is
 // kept twice and each elimination step reads one copy and writes the other, so a step is one pass and one barrier;
@@ -681,11 +850,23 @@ constexpr int tile_sy() {
 }
 
 template <int NS, bool PRE>
+void launch_rowband(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
+                    double* out, cudaStream_t s) {
+    constexpr int H = rb_halo<NS, PRE>();
+    const dim3 grid(div_up(L.w, RB_RX - 2 * H), div_up(L.h, RB_RY - 2 * H));
+    if (L.t) mg_rowband_kernel<NS, PRE, true><<<grid, RB_NT, 0, s>>>(L, C, xc, omega, part, counter, out);
+    else mg_rowband_kernel<NS, PRE, false><<<grid, RB_NT, 0, s>>>(L, C, xc, omega, part, counter, out);
+    sr_note_launch();
+}
+
+template <int NS, bool PRE>
 void launch_smooth(const MgLevel& L, const MgLevel& C, const float* xc, float omega, double* part, unsigned* counter,
                    double* out, int tile, cudaStream_t s) {
     if (tile < 0 ? small_tiles(L) : tile == 1)
         launch_smooth_t<NS, PRE, SMALL_SX, tile_sy<NS, PRE, SMALL_SX, SMALL_SY, SMALL_NT>(), SMALL_NT>(
             L, C, xc, omega, part, counter, out, s);
+    else if (L.w % 2 == 0)  // the row-band kernel loads cell pairs as 8-byte words
+        launch_rowband<NS, PRE>(L, C, xc, omega, part, counter, out, s);
     else
         launch_smooth_t<NS, PRE, BIG_SX, tile_sy<NS, PRE, BIG_SX, BIG_SY, BIG_NT>(), BIG_NT>(L, C, xc, omega, part,
                                                                                            counter, out, s);
@@ -739,9 +920,10 @@ size_t mg_smooth_ctas(int w, int h) {
     MgLevel L;
     L.w = w;
     L.h = h;
-    // a bound: the shortest tile tile_sy can pick
-    return small_tiles(L) ? (size_t)div_up(w, SMALL_SX) * div_up(h, SMALL_SY - 6)
-                          : (size_t)div_up(w, BIG_SX) * div_up(h, BIG_SY - 6);
+    // a bound: the shortest tile tile_sy can pick, or the row-band kernel's smallest output tile (V(3,3)'s pre-smoother)
+    const size_t rb = (size_t)div_up(w, RB_RX - 2 * rb_halo<6, true>()) * div_up(h, RB_RY - 2 * rb_halo<6, true>());
+    return std::max(rb, small_tiles(L) ? (size_t)div_up(w, SMALL_SX) * div_up(h, SMALL_SY - 6)
+                                       : (size_t)div_up(w, BIG_SX) * div_up(h, BIG_SY - 6));
 }
 
 void Multigrid::create(int w, int h, int pre_, int post_) {

@@ -3,8 +3,8 @@
 crates/sr-physics/src/reference/mod.rs:264-297), run on the worlds the benchmark times rather than on small ones.
 
   - the headline world: one full hydro + gravity + FLD step of the seeded 2048² world (scenes.full_step) from the
-    same f32 start as the twin: rel L1 <= 1e-5 per field, P2's field of the start state within 1e-5, and the implicit
-    solve at an FP64 relative residual <= 1e-8;
+    same f32 start as the twin: rel L1 <= 1e-5 per field, P2's potential of the start state within 1e-5 and its
+    acceleration within the reference's field bar 1e-3, and the implicit solve at an FP64 relative residual <= 1e-8;
   - config 1, Sod 512² (γ = 1.4, minmod, leave edges): one step within 1e-5 per field; 200 steps within the reference's
     G-REF bands (Σ and E rel L1 <= 1e-3, clock within 5e-4) and the exact Riemann density within 2 % in L1
     (tests/gpu/sod.rs:158-173's bar);
@@ -48,7 +48,10 @@ def test_the_2048_full_step_matches_the_twin():
     assert rep.converged and rep.rel_residual <= 1e-8, (rep.converged, rep.rel_residual)
     twin = O.Twin(cfg, P.astype(np.float64), kappa.astype(np.float64))
     ophi, ogx, ogy = twin.field()
-    assert rel_l1(phi, ophi) <= 1e-5 and rel_l1(gx, ogx) <= 1e-5 and rel_l1(gy, ogy) <= 1e-5
+    # φ to 1e-5; g to the reference's own GPU-vs-twin bar for the field, 1e-3 (tests/gpu/grav.rs:1-15): g is the
+    # central difference of an FP32 φ near -420 (one ulp 3e-5) and is itself ~0.2, so it carries ~5e-5 of rounding
+    assert rel_l1(phi, ophi) <= 1e-5, rel_l1(phi, ophi)
+    assert rel_l1(gx, ogx) <= 1e-3 and rel_l1(gy, ogy) <= 1e-3, (rel_l1(gx, ogx), rel_l1(gy, ogy))
     twin.step(1)
     ref = twin.state()
     errs = [rel_l1(gpu[k], ref[k]) for k in range(4)]
