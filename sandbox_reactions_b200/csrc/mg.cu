@@ -644,6 +644,56 @@ __device__ __forceinline__ void tail_sweep(const TailLevel T, int color) {
     __syncthreads();
 }
 
+// `count` half-sweeps from colour `color` of a tail level of at most 64 x 64 cells, each thread holding one 2 x 2 block
+// (warp v's rows 2v, 2v + 1, lane j's columns 2j, 2j + 1) with its coefficients and iterate in registers: a cell's
+// neighbours inside the block are registers, across a column edge a shuffle, across a row edge one shared-memory load
+// of the level's x (kept current after every half-sweep). Same arithmetic as tail_sweep.
+__device__ __forceinline__ void tail_sweeps_reg(const TailLevel T, int color, int count) {
+    float* f = tsf();
+    const float *b = f + T.b, *dx = f + T.dx, *dy = f + T.dy, *inv = f + T.inv;
+    float* x = f + T.x;
+    const int lane = threadIdx.x & 31, x0 = 2 * lane, y0 = 2 * (threadIdx.x >> 5);
+    float bb[4], iv[4], cl[4], cr[4], cu[4], cd[4], xv[4];
+    bool ok[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int xx = x0 + (k & 1), yy = y0 + (k >> 1);
+        ok[k] = xx < T.w && yy < T.h;
+        const int i = ok[k] ? yy * T.w + xx : 0;
+        bb[k] = ok[k] ? b[i] : 0.0f;
+        iv[k] = ok[k] ? inv[i] : 0.0f;
+        cl[k] = ok[k] && xx > 0 ? dx[i - 1] : 0.0f;
+        cr[k] = ok[k] && xx + 1 < T.w ? dx[i] : 0.0f;
+        cu[k] = ok[k] && yy > 0 ? dy[i - T.w] : 0.0f;
+        cd[k] = ok[k] && yy + 1 < T.h ? dy[i] : 0.0f;
+        xv[k] = ok[k] ? x[i] : 0.0f;
+    }
+    const int iu = y0 > 0 ? (y0 - 1) * T.w : 0, id = y0 + 2 < T.h ? (y0 + 2) * T.w : 0;
+    const bool hu = y0 > 0 && ok[0], hd = y0 + 2 < T.h && ok[2];
+    for (int s = 0; s < count; s++) {
+        if (((color + s) & 1) == 0) {  // cells (2j, 2v) and (2j + 1, 2v + 1)
+            const float left = __shfl_up_sync(0xffffffffu, xv[1], 1);
+            const float right = __shfl_down_sync(0xffffffffu, xv[2], 1);
+            const float up = hu ? x[iu + x0] : 0.0f;
+            const float down = hd && ok[3] ? x[id + x0 + 1] : 0.0f;
+            xv[0] = (bb[0] + cl[0] * left + cr[0] * xv[1] + cu[0] * up + cd[0] * xv[2]) * iv[0];
+            xv[3] = (bb[3] + cl[3] * xv[2] + cr[3] * right + cu[3] * xv[1] + cd[3] * down) * iv[3];
+            if (ok[0]) x[y0 * T.w + x0] = xv[0];
+            if (ok[3]) x[(y0 + 1) * T.w + x0 + 1] = xv[3];
+        } else {  // cells (2j + 1, 2v) and (2j, 2v + 1)
+            const float right = __shfl_down_sync(0xffffffffu, xv[0], 1);
+            const float left = __shfl_up_sync(0xffffffffu, xv[3], 1);
+            const float up = hu && ok[1] ? x[iu + x0 + 1] : 0.0f;
+            const float down = hd ? x[id + x0] : 0.0f;
+            xv[1] = (bb[1] + cl[1] * xv[0] + cr[1] * right + cu[1] * up + cd[1] * xv[3]) * iv[1];
+            xv[2] = (bb[2] + cl[2] * left + cr[2] * xv[3] + cu[2] * xv[0] + cd[2] * down) * iv[2];
+            if (ok[1]) x[y0 * T.w + x0 + 1] = xv[1];
+            if (ok[2]) x[(y0 + 1) * T.w + x0] = xv[2];
+        }
+        __syncthreads();
+    }
+}
+
 __device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel C) {
     float* f = tsf();
     const float *fc = f + F.c, *fdx = f + F.dx, *fdy = f + F.dy, *fb = f + F.b, *fx = f + F.x, *ft = f + F.t;
@@ -732,9 +782,13 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
     __syncthreads();
     for (int l = A.t; l < A.nl - 1; l++) {
         const TailLevel Tl = T[l];
-        for (int s = 0; s < A.pre; s++) {
-            tail_sweep(Tl, 0);
-            tail_sweep(Tl, 1);
+        if (Tl.w <= 64 && Tl.h <= 64) {
+            tail_sweeps_reg(Tl, 0, 2 * A.pre);
+        } else {
+            for (int s = 0; s < A.pre; s++) {
+                tail_sweep(Tl, 0);
+                tail_sweep(Tl, 1);
+            }
         }
         tail_restrict(Tl, T[l + 1]);
     }
@@ -765,9 +819,13 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
                 }
         }
         __syncthreads();
-        for (int s = 0; s < A.post; s++) {
-            tail_sweep(F, 1);
-            tail_sweep(F, 0);
+        if (F.w <= 64 && F.h <= 64) {
+            tail_sweeps_reg(F, 1, 2 * A.post);
+        } else {
+            for (int s = 0; s < A.post; s++) {
+                tail_sweep(F, 1);
+                tail_sweep(F, 0);
+            }
         }
     }
     const TailLevel top = T[A.t];
