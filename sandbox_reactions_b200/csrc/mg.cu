@@ -18,12 +18,23 @@ constexpr int SMALL_SX = 32, SMALL_SY = 16, SMALL_NT = 256;
 constexpr int TAIL_THREADS = 1024;
 constexpr int TAIL_ROWS = TAIL_THREADS / 32;  // the tail's threads as 32 columns x TAIL_ROWS rows
 
+// A tail level's arrays as offsets into the tail's shared memory (floats for the seven arrays, bytes for the mask).
+struct TailLevel {
+    int w, h;
+    int c, dx, dy, b, x, inv, t;  // float offsets; inv: the inverse diagonal (0 on masked cells); t: the weights towards
+                                  // the next coarser level
+    int m;                        // byte offset of the mask
+};
+
 struct TailArgs {
     int t, nl, pre, post;
     float omega;
-    const float* coarse_inv;  // the coarsest level's inverse, n x n
+    int sinv;                 // float offset of the coarsest level's inverse (nc x nc)
+    const float4* img;        // the tail's shared memory image (everything but the top level's b), per Newton pass
+    int img_f4;               // its size in 16-byte words
     double* out;              // non-null when the tail's top level is level 0: <b, x2> written here
     MgLevel L[kMgMaxLevels];
+    TailLevel T[kMgMaxLevels];
 };
 
 // Level 0's couplings to the +x / +y neighbours from the f64 faces, zero unless both cells are gas.
@@ -610,15 +621,9 @@ __global__ void mg_coarse_inverse_kernel(MgLevel C, float* inv) {
 }
 
 // ---- the coarse tail: every level from t on, inside one CTA
-// A level's arrays as offsets into the tail's dynamic shared memory (floats for the six arrays, bytes for the mask):
-// indexing the extern shared array itself keeps every access a shared-memory access.
+// The tail's levels live in its dynamic shared memory at the offsets of TailLevel: indexing the extern shared array
+// itself keeps every access a shared-memory access.
 extern __shared__ __align__(16) unsigned char tail_smem_raw[];
-struct TailLevel {
-    int w, h;
-    int c, dx, dy, b, x, inv, t;  // float offsets; inv: the inverse diagonal (0 on masked cells), formed once per
-                                  // launch; t: the weights towards the next coarser level
-    int m;                     // byte offset of the mask
-};
 __device__ __forceinline__ float* tsf() { return reinterpret_cast<float*>(tail_smem_raw); }
 
 // Threads of the tail run as 32 columns x TAIL_ROWS rows: thread (tx, ty) takes rows ty, ty + TAIL_ROWS, ... and, of
@@ -728,57 +733,19 @@ __device__ __forceinline__ void tail_restrict(const TailLevel F, const TailLevel
 __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
     float* f = tsf();
     __shared__ TailLevel T[kMgMaxLevels];  // indexed by a run-time level
-    // carve shared memory: six float arrays per level, the coarsest inverse, then the masks
-    int off = 0;  // in floats
-    for (int l = A.t; l < A.nl; l++) {
-        const int n = A.L[l].w * A.L[l].h;
-        if (threadIdx.x == 0) {
-            T[l].w = A.L[l].w;
-            T[l].h = A.L[l].h;
-            T[l].c = off;
-            T[l].dx = off + n;
-            T[l].dy = off + 2 * n;
-            T[l].b = off + 3 * n;
-            T[l].x = off + 4 * n;
-            T[l].inv = off + 5 * n;
-            T[l].t = off + 6 * n;
-        }
-        off += 7 * n;
-    }
-    const int nc = A.L[A.nl - 1].w * A.L[A.nl - 1].h;
-    float* sinv = f + off;  // the coarsest level's inverse, nc x nc
-    off += nc * nc;
-    int moff = off * (int)sizeof(float);  // bytes
-    for (int l = A.t; l < A.nl; l++) {
-        if (threadIdx.x == 0) T[l].m = moff;
-        moff += A.L[l].w * A.L[l].h;
-    }
+    if (threadIdx.x < kMgMaxLevels) T[threadIdx.x] = A.T[threadIdx.x];
+    // every level's coefficients, weights, inverse diagonal and mask, the iterates at 0 and the coarsest inverse, as
+    // packed once per Newton pass: one 16-byte copy per word, all in flight together
+    float4* dst = reinterpret_cast<float4*>(tail_smem_raw);
+    for (int k = threadIdx.x; k < A.img_f4; k += TAIL_THREADS) dst[k] = A.img[k];
     __syncthreads();
-    for (int k = threadIdx.x; k < nc * nc; k += TAIL_THREADS) sinv[k] = A.coarse_inv[k];
-    for (int l = A.t; l < A.nl; l++) {
-        const TailLevel Tl = T[l];
-        const int n = Tl.w * Tl.h;
-        for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
-            f[Tl.c + i] = A.L[l].c[i];
-            f[Tl.dx + i] = A.L[l].dx[i];
-            f[Tl.dy + i] = A.L[l].dy[i];
-            tail_smem_raw[Tl.m + i] = A.L[l].mask[i];
-            f[Tl.x + i] = 0.0f;
-            f[Tl.t + i] = l + 1 < A.nl ? (A.L[l].t ? A.L[l].t[i] : 1.0f) : 0.0f;
-            if (l == A.t) f[Tl.b + i] = A.L[l].b[i];
-        }
+    {
+        const int n = T[A.t].w * T[A.t].h;
+        const float* b = A.L[A.t].b;
+        for (int i = threadIdx.x; i < n; i += TAIL_THREADS) f[T[A.t].b + i] = b[i];
     }
-    __syncthreads();
-    for (int l = A.t; l < A.nl; l++) {
-        const TailLevel Tl = T[l];
-        const int n = Tl.w * Tl.h;
-        for (int i = threadIdx.x; i < n; i += TAIL_THREADS) {
-            const int x = i % Tl.w, y = i / Tl.w;
-            const float d = f[Tl.c + i] + f[Tl.dx + i] + f[Tl.dy + i] + (x > 0 ? f[Tl.dx + i - 1] : 0.0f) +
-                            (y > 0 ? f[Tl.dy + i - Tl.w] : 0.0f);
-            f[Tl.inv + i] = tail_smem_raw[Tl.m + i] ? 1.0f / d : 0.0f;
-        }
-    }
+    const int nc = T[A.nl - 1].w * T[A.nl - 1].h;
+    const float* sinv = f + A.sinv;
     __syncthreads();
     for (int l = A.t; l < A.nl - 1; l++) {
         const TailLevel Tl = T[l];
@@ -850,12 +817,86 @@ __global__ void __launch_bounds__(TAIL_THREADS) mg_tail_kernel(TailArgs A) {
     }
 }
 
+// The tail's shared-memory layout: seven float arrays per level, the coarsest inverse, then the masks; the byte size
+// rounded up to 16. Fills A.T, A.sinv and A.img_f4.
+size_t tail_layout(const Multigrid& M, TailArgs& A) {
+    int off = 0;  // floats
+    for (int l = M.tail; l < M.nlevels; l++) {
+        const int n = M.L[l].w * M.L[l].h;
+        TailLevel& T = A.T[l];
+        T.w = M.L[l].w;
+        T.h = M.L[l].h;
+        T.c = off;
+        T.dx = off + n;
+        T.dy = off + 2 * n;
+        T.b = off + 3 * n;
+        T.x = off + 4 * n;
+        T.inv = off + 5 * n;
+        T.t = off + 6 * n;
+        off += 7 * n;
+    }
+    const int nc = M.L[M.nlevels - 1].w * M.L[M.nlevels - 1].h;
+    A.sinv = off;
+    off += nc * nc;
+    int moff = off * (int)sizeof(float);
+    for (int l = M.tail; l < M.nlevels; l++) {
+        A.T[l].m = moff;
+        moff += M.L[l].w * M.L[l].h;
+    }
+    const size_t bytes = ((size_t)moff + 15) & ~(size_t)15;
+    A.img_f4 = (int)(bytes / 16);
+    return bytes;
+}
+
 size_t tail_smem(const Multigrid& M) {
-    size_t s = 0;
-    for (int l = M.tail; l < M.nlevels; l++) s += (size_t)M.L[l].w * M.L[l].h * (7 * sizeof(float) + 1);
-    const size_t nc = (size_t)M.L[M.nlevels - 1].w * M.L[M.nlevels - 1].h;
-    s += sizeof(float) * nc * nc;
-    return (s + 15) & ~(size_t)15;
+    TailArgs A;
+    return tail_layout(M, A);
+}
+
+// Everything the tail kernel and its packing need but the output slot.
+size_t tail_args(const Multigrid& M, TailArgs& T) {
+    const size_t bytes = tail_layout(M, T);
+    T.t = M.tail;
+    T.nl = M.nlevels;
+    T.pre = M.pre;
+    T.post = M.post;
+    T.omega = M.omega;
+    T.img = reinterpret_cast<const float4*>(M.tail_img);
+    T.out = nullptr;
+    for (int l = 0; l < M.nlevels; l++) T.L[l] = M.L[l];
+    return bytes;
+}
+
+// The tail's image for the next V-cycles (once per Newton pass, after the coarsening): each tail level's c, dx, dy,
+// inverse diagonal, weights and mask at their offsets, b and x at 0, the coarsest inverse, and the padding after the
+// masks at 0. Every byte of the image is written by exactly one thread.
+__global__ void mg_tail_pack_kernel(TailArgs A, const float* __restrict__ coarse_inv, float* img) {
+    unsigned char* bytes = reinterpret_cast<unsigned char*>(img);
+    const int stride = gridDim.x * blockDim.x, tid = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int l = A.t; l < A.nl; l++) {
+        const TailLevel T = A.T[l];
+        const MgLevel& L = A.L[l];
+        const int n = T.w * T.h;
+        for (int i = tid; i < n; i += stride) {
+            const int x = i % T.w, y = i / T.w;
+            const float c = L.c[i], dx = L.dx[i], dy = L.dy[i];
+            const float d = c + dx + dy + (x > 0 ? L.dx[i - 1] : 0.0f) + (y > 0 ? L.dy[i - T.w] : 0.0f);
+            const uint8_t m = L.mask[i];
+            img[T.c + i] = c;
+            img[T.dx + i] = dx;
+            img[T.dy + i] = dy;
+            img[T.b + i] = 0.0f;
+            img[T.x + i] = 0.0f;
+            img[T.inv + i] = m ? 1.0f / d : 0.0f;
+            img[T.t + i] = l + 1 < A.nl ? (L.t ? L.t[i] : 1.0f) : 0.0f;
+            bytes[T.m + i] = m;
+        }
+    }
+    const TailLevel last = A.T[A.nl - 1];
+    const int nc = last.w * last.h;
+    for (int k = tid; k < nc * nc; k += stride) img[A.sinv + k] = coarse_inv[k];
+    const int end = last.m + nc;
+    for (int k = end + tid; k < A.img_f4 * 16; k += stride) bytes[k] = 0;
 }
 
 template <int NS, bool PRE, int SX, int SY, int NT, bool VEC, bool WT>
@@ -1018,6 +1059,7 @@ void Multigrid::create(int w, int h, int pre_, int post_) {
     const size_t nc = (size_t)L[nlevels - 1].w * L[nlevels - 1].h;
     SR_REQUIRE(nc <= 64, "the coarsest level holds more than 64 cells");
     SR_CUDA_TRY(cudaMalloc(&coarse_inv, sizeof(float) * nc * nc));
+    SR_CUDA_TRY(cudaMalloc(&tail_img, ts));
     SR_CUDA_TRY(cudaFuncSetAttribute(mg_coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(2 * nc * 2 * nc * sizeof(double))));
     set_attributes_ns<2>();
@@ -1041,6 +1083,8 @@ void Multigrid::destroy() {
     }
     cudaFree(coarse_inv);
     coarse_inv = nullptr;
+    cudaFree(tail_img);
+    tail_img = nullptr;
     nlevels = 0;
 }
 
@@ -1121,6 +1165,10 @@ void Multigrid::coarsen(cudaStream_t s) {
     const size_t nc = (size_t)C.w * C.h;
     mg_coarse_inverse_kernel<<<1, 1024, 2 * nc * 2 * nc * sizeof(double), s>>>(C, coarse_inv);
     sr_note_launch();
+    TailArgs T;
+    tail_args(*this, T);
+    mg_tail_pack_kernel<<<8, 256, 0, s>>>(T, coarse_inv, tail_img);
+    sr_note_launch();
     if (!tuned) autotune(s);
 }
 
@@ -1130,15 +1178,9 @@ void Multigrid::apply(const float* r, float* z, double* part, unsigned* counter,
     for (int l = 0; l < tail; l++)
         smooth(pre, true, L[l], L[l + 1], nullptr, omega, nullptr, nullptr, nullptr, s, tile[l]);
     TailArgs T;
-    T.coarse_inv = coarse_inv;
-    T.t = tail;
-    T.nl = nlevels;
-    T.pre = pre;
-    T.post = post;
-    T.omega = omega;
+    const size_t ts = tail_args(*this, T);
     T.out = tail == 0 ? rz_out : nullptr;
-    for (int l = 0; l < nlevels; l++) T.L[l] = L[l];
-    mg_tail_kernel<<<1, TAIL_THREADS, tail_smem(*this), s>>>(T);
+    mg_tail_kernel<<<1, TAIL_THREADS, ts, s>>>(T);
     sr_note_launch();
     for (int l = tail - 1; l >= 0; l--)
         smooth(post, false, L[l], L[l + 1], L[l + 1].x2, omega, l == 0 ? part : nullptr, l == 0 ? counter : nullptr,

@@ -42,6 +42,8 @@ struct Multigrid {
     float omega = 1.0f;  // coarse-correction weight
     MgLevel L[kMgMaxLevels];
     float* coarse_inv = nullptr;  // the coarsest level's operator inverted (at most 64 x 64), per Newton pass
+    float* tail_img = nullptr;    // the coarse tail's shared-memory image (coefficients, inverse diagonals, weights,
+                                  // masks, the coarsest inverse), packed once per Newton pass
 
     void create(int w, int h, int pre, int post);
     void destroy();
