@@ -48,6 +48,24 @@ struct Face {
     Prim p;      // the primitives it stands for
 };
 
+// Division and the square root of a non-negative value at the hardware's approximate rate on the device (one
+// reciprocal or reciprocal square root and a product, within 2 ulp; the FP32 physics is held to 1e-5 of the f64
+// twin), exact on the host.
+SR_HOST_DEVICE float sr_div(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+SR_HOST_DEVICE float sr_sqrt(float x) {
+#ifdef __CUDA_ARCH__
+    return x > 0.0f ? x * rsqrtf(x) : 0.0f;
+#else
+    return x > 0.0f ? sqrtf(x) : 0.0f;
+#endif
+}
+
 SR_HOST_DEVICE float eos_pi(const HydroConst& H, float s, float eps) { return H.gm1 * s * eps; }
 
 // A cell as primitives (reference hydro.rs:424-441): the floor state below Σ_vac, else ε_th floored at T_floor/(μ(γ-1)).
@@ -60,7 +78,7 @@ SR_HOST_DEVICE Prim eos_read(const HydroConst& H, float s, float mx, float my, f
         p.p = eos_pi(H, H.sigma_floor, H.eps_floor);
         return p;
     }
-    const float rs = 1.0f / s;  // one division per cell: the velocities and ε by products
+    const float rs = sr_div(1.0f, s);  // one division per cell: the velocities and ε by products
     p.u = mx * rs;
     p.v = my * rs;
     float raw = E * rs - 0.5f * (p.u * p.u + p.v * p.v);
@@ -72,7 +90,7 @@ SR_HOST_DEVICE Prim eos_read(const HydroConst& H, float s, float mx, float my, f
 
 // The conserved vector of primitives (hydro.rs:443-460).
 SR_HOST_DEVICE void eos_cons(const HydroConst& H, const Prim& p, float* U) {
-    float thermal = p.p / p.s * H.inv_gm1;
+    float thermal = sr_div(p.p, p.s) * H.inv_gm1;
     float eps = fmaxf(thermal, H.eps_floor);
     U[0] = p.s;
     U[1] = p.s * p.u;
@@ -80,15 +98,19 @@ SR_HOST_DEVICE void eos_cons(const HydroConst& H, const Prim& p, float* U) {
     U[3] = p.s * eps + 0.5f * p.s * (p.u * p.u + p.v * p.v);
 }
 
-// The primitives of a conserved vector, false when it is no state (hydro.rs:462-478).
+// The primitives of a conserved vector, false when it is no state (hydro.rs:462-478): Σ not positive, any component
+// not finite, or no thermal energy left. The finiteness test rides on the derived values: a non-finite Σu or Σv makes
+// u or v, hence the thermal energy, -inf or NaN; a non-finite E makes it ±inf or NaN; Σ = +inf makes every velocity 0
+// (or NaN) and the thermal energy 0 (or NaN) — so "thermal energy positive and finite" rejects the states with a
+// non-finite component, as the reference's test of all four does (and, beyond it, a state whose thermal energy per mass
+// alone overflows FP32, which no FP32 cell can hold anyway).
 SR_HOST_DEVICE bool eos_prim(const HydroConst& H, const float* U, Prim& out) {
     float s = U[0];
     if (!(s > 0.0f)) return false;  // NaN or <= 0
-    if (!(isfinite(U[0]) && isfinite(U[1]) && isfinite(U[2]) && isfinite(U[3]))) return false;
-    const float rs = 1.0f / s;  // one division per state: the velocities and ε by products
+    const float rs = sr_div(1.0f, s);  // one division per state: the velocities and ε by products
     const float u = U[1] * rs, v = U[2] * rs;
     float raw = U[3] * rs - 0.5f * (u * u + v * v);
-    if (!(raw > 0.0f)) return false;
+    if (!(raw > 0.0f) || raw == INFINITY) return false;
     float eps = fmaxf(raw, H.eps_floor);
     out.s = s;
     out.u = u;
@@ -98,8 +120,7 @@ SR_HOST_DEVICE bool eos_prim(const HydroConst& H, const float* U, Prim& out) {
 }
 
 SR_HOST_DEVICE float eos_sound(const HydroConst& H, const Prim& p) {
-    float c2 = H.gamma * p.p / p.s;
-    return sqrtf(fmaxf(c2, 0.0f));
+    return sr_sqrt(H.gamma * sr_div(p.p, p.s));
 }
 
 // The Euler flux through a face normal to `dir` (hydro.rs:485-499).

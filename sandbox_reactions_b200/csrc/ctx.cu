@@ -47,6 +47,7 @@ struct sr_ctx {
     float* part_best = nullptr;
     int* part_idx = nullptr;
     double* hreport = nullptr;  // 7 doubles
+    int* herr = nullptr;        // the hydro kernels' error flag (a bounded wait gave up)
     DtRecord* rec = nullptr;
     float *part_rate = nullptr, *part_g = nullptr;
     long long* part_nf = nullptr;
@@ -112,7 +113,7 @@ static void ctx_free(sr_ctx* c) {
     cudaFree(c->src); cudaFree(c->phim); cudaFree(c->gxm); cudaFree(c->gym);
     cudaFree(c->kappa);
     if (c->grav_ready) c->grav.destroy();
-    cudaFree(c->part_d); cudaFree(c->part_best); cudaFree(c->part_idx); cudaFree(c->hreport);
+    cudaFree(c->part_d); cudaFree(c->part_best); cudaFree(c->part_idx); cudaFree(c->hreport); cudaFree(c->herr);
     cudaFree(c->rec); cudaFree(c->part_rate); cudaFree(c->part_g); cudaFree(c->part_nf);
     if (c->heat) heat_destroy(c->heat);
     for (auto e : c->events) cudaEventDestroy(e);
@@ -190,6 +191,7 @@ static HydroArgs hydro_args(sr_ctx* c) {
     A.part_best = c->part_best;
     A.part_idx = c->part_idx;
     A.report = c->hreport;
+    A.err = c->herr;
     return A;
 }
 
@@ -336,6 +338,7 @@ sr_status sr_create(const sr_config* cfg, sr_ctx** out) {
         dalloc(&c->part_best, (size_t)hb);
         dalloc(&c->part_idx, (size_t)hb);
         dalloc(&c->hreport, 7);
+        dalloc(&c->herr, 1);
         dalloc(&c->rec, 1);
         int fb = floors_dt_blocks(c->w, c->h);
         dalloc(&c->part_rate, (size_t)fb);
@@ -393,6 +396,12 @@ sr_status sr_step(sr_ctx* c, uint32_t steps) {
         SR_REQUIRE(c->uploaded, "sr_step: no state uploaded");
         run_steps(c, steps);
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        int herr = 0;
+        SR_CUDA_TRY(cudaMemcpy(&herr, c->herr, sizeof herr, cudaMemcpyDeviceToHost));
+        if (herr) {
+            SR_CUDA_TRY(cudaMemset(c->herr, 0, sizeof herr));
+            throw SrError{SR_E_TIMEOUT, "a TMA wait of the hydro kernel gave up"};
+        }
         if (c->cfg.precond == SR_PRECOND_LEARNED && c->learner && learned_error(c->learner->L, c->stream))
             throw SrError{SR_E_TIMEOUT, "a tensor-core wait of the learned preconditioner gave up"};
     });

@@ -1,20 +1,22 @@
-// hydro.cu — P4, the MUSCL-Hancock/HLL gas step, as one shared-memory tiled stencil kernel per pass (sm_100a, FP32).
+// hydro.cu — P4, the MUSCL-Hancock/HLL gas step, as one tiled stencil kernel per pass (sm_100a, FP32).
 //
-// One CTA owns a TX x TY tile of output cells. It stages the primitives of the tile grown by two cells (the
-// reconstruction's reach, ghosts of the world's edges included) in shared memory once, runs the Hancock predictor for
-// the tile and for the one-cell strips around it, exchanges the predicted faces through shared memory for the HLL
-// fluxes, and finishes with the per-cell epilogue of its pass:
+// One CTA owns a tile of output cells; the tile grown by two cells (the reconstruction's reach) arrives in shared
+// memory by one TMA box, the world's ghosts are formed there, every lane runs the Hancock predictor for one cell (the
+// tile's and the one-cell ring around it), the faces meet for the HLL fluxes by warp shuffles (x) and shared memory
+// (y), and the per-cell epilogue of the pass finishes:
 //   - kHydroUpdate:     U' = U - Δt ΔF (no gravity);
 //   - kHydroSource:     the half step's gravity source ½(Σⁿ + Σⁿ⁺¹), masked (reference hydro.rs:815-836);
 //   - kHydroUpdateGrav: U' with gravity's half-step kick and the faces' work across φ_mid (hydro.rs:871-947).
 // The scheme follows crates/sr-physics/src/reference/hydro.rs (step_held without held cells, sinks or radiation).
 #include "hydro.cuh"
 
-namespace {
+#include <cudaTypedefs.h>
 
-constexpr int TX = kHydroTileX, TY = kHydroTileY;
-constexpr int EX = TX + 4, EY = TY + 4;  // the staged region: the tile grown by 2
-constexpr int NT = TX * TY;              // threads per CTA: one per tile cell
+#include <string>
+
+#include "tma.cuh"
+
+namespace {
 
 __device__ __forceinline__ float lim_mc(float l, float c, float r) {
     float a = c - l, b = r - c;
@@ -28,20 +30,21 @@ __device__ __forceinline__ float lim_minmod(float l, float c, float r) {
     return copysignf(fminf(fabsf(a), fabsf(b)), a);
 }
 
-__device__ __forceinline__ float lim(int which, float l, float c, float r) {
-    return which == SR_LIMITER_MINMOD ? lim_minmod(l, c, r) : lim_mc(l, c, r);
+template <int LIM>
+__device__ __forceinline__ float lim(float l, float c, float r) {
+    return LIM == SR_LIMITER_MINMOD ? lim_minmod(l, c, r) : lim_mc(l, c, r);
 }
 
 // Limited slopes of (Σ, u, v, Π) along one axis; Σ and Π flat where the thermal bracket refuses a face
-// (hydro.rs:293-331, HOT_FACE = 2).
-__device__ __forceinline__ Prim slope(const HydroConst& H, const Prim& l, const Prim& c, const Prim& r, float ql,
-                                      float qc, float qr) {
+// (hydro.rs:293-331, HOT_FACE = 2). The limiter and the bracket are the kernel's template parameters.
+template <int LIM, bool BRACKET>
+__device__ __forceinline__ Prim slope(const Prim& l, const Prim& c, const Prim& r, float ql, float qc, float qr) {
     Prim s;
-    s.s = lim(H.limiter, l.s, c.s, r.s);
-    s.u = lim(H.limiter, l.u, c.u, r.u);
-    s.v = lim(H.limiter, l.v, c.v, r.v);
-    s.p = lim(H.limiter, l.p, c.p, r.p);
-    if (H.bracket) {
+    s.s = lim<LIM>(l.s, c.s, r.s);
+    s.u = lim<LIM>(l.u, c.u, r.u);
+    s.v = lim<LIM>(l.v, c.v, r.v);
+    s.p = lim<LIM>(l.p, c.p, r.p);
+    if (BRACKET) {
         float hottest = fmaxf(fmaxf(ql, qc), qr);  // Π/Σ of the three cells, staged once per cell
         float plo = c.p - 0.5f * s.p, blo = 2.0f * hottest * (c.s - 0.5f * s.s);
         float phi = c.p + 0.5f * s.p, bhi = 2.0f * hottest * (c.s + 0.5f * s.s);
@@ -62,103 +65,22 @@ __device__ __forceinline__ Prim offset(const Prim& c, const Prim& s, float f) {
     return o;
 }
 
-// A face advanced by the Hancock increment, or the unevolved face when the advanced one is no state (hydro.rs:501-513).
-__device__ __forceinline__ void evolved(const HydroConst& H, const Prim& base, const float* u0, const float* d, Face& F) {
-    float U[4] = {u0[0] + d[0], u0[1] + d[1], u0[2] + d[2], u0[3] + d[3]};
-    Prim p;
-    if (eos_prim(H, U, p)) {
-        F.U[0] = U[0]; F.U[1] = U[1]; F.U[2] = U[2]; F.U[3] = U[3];
-        F.p = p;
-    } else {
-        F.U[0] = u0[0]; F.U[1] = u0[1]; F.U[2] = u0[2]; F.U[3] = u0[3];
-        F.p = base;
-    }
-}
-
-// The four predicted faces [x-, x+, y-, y+] of a cell and its centre's (Σ, Σu, Σv) half a step on (hydro.rs:587-614).
-// `want` is a bit mask of the faces the caller keeps.
-__device__ __forceinline__ void predict(const HydroConst& H, const Prim& l, const Prim& c, const Prim& r,
-                                        const Prim& up, const Prim& dn, const float* q, float half, bool grav,
-                                        float gx, float gy, int want, Face* out, float* mid) {
-    // q: Π/Σ of l, c, r, up, dn
-    Prim sx = slope(H, l, c, r, q[0], q[1], q[2]);
-    Prim sy = slope(H, up, c, dn, q[3], q[1], q[4]);
-    Prim wf[4] = {offset(c, sx, -0.5f), offset(c, sx, 0.5f), offset(c, sy, -0.5f), offset(c, sy, 0.5f)};
-    float uf[4][4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) eos_cons(H, wf[k], uf[k]);
-    float fxl[4], fxr[4], fyl[4], fyr[4];
-    euler_flux(wf[0], uf[0][3], 0, fxl);
-    euler_flux(wf[1], uf[1][3], 0, fxr);
-    euler_flux(wf[2], uf[2][3], 1, fyl);
-    euler_flux(wf[3], uf[3][3], 1, fyr);
-    float delta[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) delta[k] = half * ((fxl[k] - fxr[k]) + (fyl[k] - fyr[k]));
-    mid[0] = c.s + delta[0];
-    mid[1] = c.s * c.u + delta[1];
-    mid[2] = c.s * c.v + delta[2];
-    if (grav) {
-        mid[1] += half * c.s * gx;
-        mid[2] += half * c.s * gy;
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        if (!(want & (1 << k))) continue;
-        float d[4] = {delta[0], delta[1], delta[2], delta[3]};
-        if (grav) {
-            const Prim& p = wf[k];
-            d[1] += half * p.s * gx;
-            d[2] += half * p.s * gy;
-            d[3] += half * p.s * ((p.u + 0.5f * half * gx) * gx + (p.v + 0.5f * half * gy) * gy);
-        }
-        evolved(H, wf[k], uf[k], d, out[k]);
-    }
-}
-
-// HLL with Davis speeds across a face normal to `dir` (hydro.rs:516-540).
-__device__ __forceinline__ void hll(const HydroConst& H, const Face& l, const Face& r, int dir, float* f) {
-    float unl = dir == 0 ? l.p.u : l.p.v, unr = dir == 0 ? r.p.u : r.p.v;
-    float cl = eos_sound(H, l.p), cr = eos_sound(H, r.p);
-    float s_l = fminf(unl - cl, unr - cr);
-    float s_r = fmaxf(unl + cl, unr + cr);
-    float fl[4], fr[4];
-    euler_flux(l.p, l.U[3], dir, fl);
-    euler_flux(r.p, r.U[3], dir, fr);
-    if (s_l >= 0.0f) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) f[k] = fl[k];
-    } else if (s_r <= 0.0f) {
-#pragma unroll
-        for (int k = 0; k < 4; k++) f[k] = fr[k];
-    } else {
-        float inv = 1.0f / (s_r - s_l);
-#pragma unroll
-        for (int k = 0; k < 4; k++) f[k] = (s_r * fl[k] - s_l * fr[k] + s_l * s_r * (r.U[k] - l.U[k])) * inv;
-    }
-}
-
-__device__ __forceinline__ void wall(const Face& own, int dir, float* f) {  // hydro.rs:556-562
-    f[0] = 0.0f; f[1] = 0.0f; f[2] = 0.0f; f[3] = 0.0f;
-    f[1 + dir] = own.p.p;
-}
-
 // Gravity's source at one face over the step (hydro.rs:1042-1067): [impulse to the low cell, low energy, high energy].
 __device__ __forceinline__ void face_work(float q, float sl, float sh, float pl, float ph, float d, float dt, float* o) {
     float a = fmaxf(sl, 0.0f), b = fmaxf(sh, 0.0f);
-    float w = a + b > 0.0f ? a / (a + b) : 0.5f;
+    float w = a + b > 0.0f ? sr_div(a, a + b) : 0.5f;
     float extra = dt * (q - 0.5f * (pl + ph)) * d;
     float c = 0.0f, kick = 0.0f, el = 0.0f, eh = 0.0f;
     if (extra < 0.0f && a > 0.0f && b > 0.0f) {
-        float ul = pl / a, uh = ph / b;
+        float ul = sr_div(pl, a), uh = sr_div(ph, b);
         float du = ul - uh;
-        float inv = 1.0f / a + 1.0f / b;
-        c = fminf(-extra, 0.25f * du * du / inv);
+        float inv = sr_div(1.0f, a) + sr_div(1.0f, b);
+        c = fminf(-extra, sr_div(0.25f * du * du, inv));
         if (c > 0.0f) {
-            float disc = sqrtf(fmaxf(du * du - 2.0f * inv * c, 0.0f));
-            kick = -2.0f * c / (du + copysignf(1.0f, du) * disc);
-            el = ul * kick + 0.5f * kick * kick / a;
-            eh = -uh * kick + 0.5f * kick * kick / b;
+            float disc = sr_sqrt(du * du - 2.0f * inv * c);
+            kick = sr_div(-2.0f * c, du + copysignf(1.0f, du) * disc);
+            el = ul * kick + sr_div(0.5f * kick * kick, a);
+            eh = -uh * kick + sr_div(0.5f * kick * kick, b);
         }
     }
     float rest = extra + c;
@@ -167,205 +89,311 @@ __device__ __forceinline__ void face_work(float q, float sl, float sh, float pl,
     o[2] = 0.5f * dt * ph * d + (1.0f - w) * rest + eh;
 }
 
-struct __align__(16) Shared {
-    float4 P[EY][EX];         // primitives (Σ, u, v, Π) of the staged region, ghosts included
-    float S[EY][EX];          // raw Σ of the staged region (out-of-world: -1, read as vacuum)
-    float Q[EY][EX];          // Π/Σ of the staged region (the thermal bracket's temperatures)
-    Face F[4][TY][TX];        // the tile's predicted faces
-    Face FL[TY], FR[TY];      // x+ faces of the column left of the tile, x- faces of the column right of it
-    Face FT[TX], FB[TX];      // y+ faces of the row above, y- faces of the row below
-    float M[TY + 2][TX + 2][3];  // half-step (Σ, Σu, Σv) of the tile and its ring
-    float FX[TY][TX + 1][4];  // x-face fluxes
-    float FY[TY + 1][TX][4];  // y-face fluxes
+// ---- the band kernel: one warp per row of the tile, one lane per cell
+//
+// A CTA covers HB_TX x HB_TY output cells with HB_W = HB_TY + 2 warps of 32 lanes: warp r is the row y0 - 1 + r and
+// lane l the column x0 - 1 + l, so the ring of cells around the tile (whose faces toward the tile the fluxes need) is
+// computed by the same straight-line code as the tile itself: lanes 0 and 31 and warps 0 and HB_W - 1 predict but
+// write nothing. The four planes of the tile grown by two cells (the reconstruction's reach) arrive in one TMA box;
+// the world's ghosts (hydro.rs:686-709) are formed from it in shared memory. Each lane predicts its cell's four faces
+// (hydro.rs:587-614); the x faces meet by warp shuffles (a lane's x+ face against the next lane's x- face), the y faces
+// through shared memory (a row's y+ faces against the next row's y- faces); the fluxes go back the same ways.
+constexpr int HB_TX = 30, HB_TY = 14, HB_W = HB_TY + 2, HB_NT = 32 * HB_W;
+constexpr int HB_SX = HB_TX + 4, HB_SY = HB_TY + 4;  // the staged region: the tile grown by 2
+constexpr int HB_BX = 40, HB_BY = HB_SY;             // the TMA box: from a 16-byte aligned column, wide enough
+constexpr uint32_t kHydroWaitPolls = 1u << 24;       // an mbarrier wait gives up after this many polls
+
+// A predicted face: its conserved vector and the primitives it stands for (Σ is U0).
+struct FaceS {
+    float U0, U1, U2, U3, u, v, P;
 };
 
-// The primitives at world position (x, y), a ghost past the world's edge (hydro.rs:686-709): bounce mirrors the
-// cells beyond with the normal velocity negated, leave copies the edge cell with it clamped outward.
-__device__ __forceinline__ Prim ghosted(const HydroConst& H, const float* __restrict__ U, int x, int y, float& raw) {
-    const int w = H.w, h = H.h;
-    const size_t n = (size_t)w * h;
-    bool xo = x < 0 || x >= w, yo = y < 0 || y >= h;
-    int cx, cy;
-    if (H.edge == SR_EDGE_BOUNCE) {
-        cx = x < 0 ? -x - 1 : (x >= w ? 2 * w - 1 - x : x);
-        cy = y < 0 ? -y - 1 : (y >= h ? 2 * h - 1 - y : y);
-    } else {
-        cx = min(max(x, 0), w - 1);
-        cy = min(max(y, 0), h - 1);
-    }
-    size_t i = (size_t)cy * w + cx;
-    float s = U[i];
-    Prim p = eos_read(H, s, U[n + i], U[2 * n + i], U[3 * n + i]);
-    raw = (xo || yo) ? -1.0f : s;
-    if (H.edge == SR_EDGE_BOUNCE) {
-        if (xo) p.u = -p.u;
-        if (yo) p.v = -p.v;
-    } else {
-        if (x < 0) p.u = fminf(p.u, 0.0f);
-        if (x >= w) p.u = fmaxf(p.u, 0.0f);
-        if (y < 0) p.v = fminf(p.v, 0.0f);
-        if (y >= h) p.v = fmaxf(p.v, 0.0f);
-    }
-    return p;
-}
+struct __align__(128) BandShared {
+    float raw[4][HB_BY][HB_BX];  // the TMA box of Σ, Σu, Σv, E (first: 128-byte aligned)
+    float4 P[HB_SY][HB_SX];      // primitives (Σ, u, v, Π) of the staged region, ghosts included
+    float Q[HB_SY][HB_SX];       // Π/Σ (the thermal bracket's temperatures)
+    float S[HB_SY][HB_SX];       // raw Σ (out of the world: -1, read as vacuum)
+    float M[3][HB_W][32];        // half-step (Σ, Σu, Σv) of each lane's cell
+    float YF[7][HB_W][32];       // each lane's y+ face
+    float FY[4][HB_W][32];       // the flux through each lane's top face
+    double red_d[6][HB_W];
+    float red_best[HB_W];
+    int red_idx[HB_W];
+    uint64_t mbar;
+};
 
-__device__ __forceinline__ Prim P_at(const Shared& sh, int ly, int lx) {
-    float4 q = sh.P[ly][lx];
+__device__ __forceinline__ Prim prim_at(const BandShared& sh, int y, int x) {
+    const float4 q = sh.P[y][x];
     Prim p;
     p.s = q.x; p.u = q.y; p.v = q.z; p.p = q.w;
     return p;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 CTAs per SM: 80 registers, ~15 B spilled
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Shared& sh = *reinterpret_cast<Shared*>(smem_raw);
+// The Euler flux of the unevolved face c + f s normal to `dir` (the Hancock increment's terms).
+__device__ __forceinline__ void face_flux(const HydroConst& H, const Prim& c, const Prim& s, float f, int dir,
+                                          float* out) {
+    const Prim wf = offset(c, s, f);
+    float uf[4];
+    eos_cons(H, wf, uf);
+    euler_flux(wf, uf[3], dir, out);
+}
+
+// The face c + f s advanced by the Hancock increment and gravity's half-kick, or unevolved when the advanced one is no
+// state (hydro.rs:501-513, 587-614).
+__device__ __forceinline__ FaceS face_state(const HydroConst& H, const Prim& c, const Prim& s, float f,
+                                            const float* delta, float half, bool grav, float gx, float gy) {
+    const Prim wf = offset(c, s, f);
+    float uf[4];
+    eos_cons(H, wf, uf);
+    float d[4] = {delta[0], delta[1], delta[2], delta[3]};
+    if (grav) {
+        d[1] += half * wf.s * gx;
+        d[2] += half * wf.s * gy;
+        d[3] += half * wf.s * ((wf.u + 0.5f * half * gx) * gx + (wf.v + 0.5f * half * gy) * gy);
+    }
+    const float U[4] = {uf[0] + d[0], uf[1] + d[1], uf[2] + d[2], uf[3] + d[3]};
+    Prim p;
+    FaceS F;
+    if (eos_prim(H, U, p)) {
+        F.U0 = U[0]; F.U1 = U[1]; F.U2 = U[2]; F.U3 = U[3];
+        F.u = p.u; F.v = p.v; F.P = p.p;
+    } else {
+        F.U0 = uf[0]; F.U1 = uf[1]; F.U2 = uf[2]; F.U3 = uf[3];
+        F.u = wf.u; F.v = wf.v; F.P = wf.p;
+    }
+    return F;
+}
+
+__device__ __forceinline__ FaceS shfl_face_down(const FaceS& F) {
+    FaceS R;
+    R.U0 = __shfl_down_sync(0xffffffffu, F.U0, 1);
+    R.U1 = __shfl_down_sync(0xffffffffu, F.U1, 1);
+    R.U2 = __shfl_down_sync(0xffffffffu, F.U2, 1);
+    R.U3 = __shfl_down_sync(0xffffffffu, F.U3, 1);
+    R.u = __shfl_down_sync(0xffffffffu, F.u, 1);
+    R.v = __shfl_down_sync(0xffffffffu, F.v, 1);
+    R.P = __shfl_down_sync(0xffffffffu, F.P, 1);
+    return R;
+}
+
+__device__ __forceinline__ void flux_of(const FaceS& F, int dir, float* f) {
+    Prim p;
+    p.s = F.U0; p.u = F.u; p.v = F.v; p.p = F.P;
+    euler_flux(p, F.U3, dir, f);
+}
+
+// HLL with Davis speeds across a face normal to `dir` (hydro.rs:516-540).
+__device__ __forceinline__ void hll_s(const HydroConst& H, const FaceS& l, const FaceS& r, int dir, float* f) {
+    const float unl = dir == 0 ? l.u : l.v, unr = dir == 0 ? r.u : r.v;
+    const float cl = sr_sqrt(H.gamma * sr_div(l.P, l.U0)), cr = sr_sqrt(H.gamma * sr_div(r.P, r.U0));
+    const float s_l = fminf(unl - cl, unr - cr);
+    const float s_r = fmaxf(unl + cl, unr + cr);
+    float fl[4], fr[4];
+    flux_of(l, dir, fl);
+    flux_of(r, dir, fr);
+    if (s_l >= 0.0f) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) f[k] = fl[k];
+    } else if (s_r <= 0.0f) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) f[k] = fr[k];
+    } else {
+        const float inv = sr_div(1.0f, s_r - s_l);
+        const float dU[4] = {r.U0 - l.U0, r.U1 - l.U1, r.U2 - l.U2, r.U3 - l.U3};
+#pragma unroll
+        for (int k = 0; k < 4; k++) f[k] = (s_r * fl[k] - s_l * fr[k] + s_l * s_r * dU[k]) * inv;
+    }
+}
+
+__device__ __forceinline__ void wall_s(const FaceS& own, int dir, float* f) {  // hydro.rs:556-562
+    f[0] = 0.0f; f[1] = 0.0f; f[2] = 0.0f; f[3] = 0.0f;
+    f[1 + dir] = own.P;
+}
+
+// The flux through face `at` (along `dir`) of the world (0 and `edge` are its walls; hydro.rs:564-582, 744-775),
+// between the faces L and R; zero for a face outside the world (`inside` false).
+__device__ __forceinline__ void face_flux_at(const HydroConst& H, const FaceS& L, const FaceS& R, int dir, int at,
+                                             int edge, bool inside, float* f) {
+    if (!inside || at < 0 || at > edge) {
+        f[0] = f[1] = f[2] = f[3] = 0.0f;
+    } else if (at == 0) {
+        if (H.edge == SR_EDGE_BOUNCE) {
+            wall_s(R, dir, f);
+        } else {
+            hll_s(H, L, R, dir, f);
+            if (f[0] > 0.0f) wall_s(R, dir, f);
+        }
+    } else if (at == edge) {
+        if (H.edge == SR_EDGE_BOUNCE) {
+            wall_s(L, dir, f);
+        } else {
+            hll_s(H, L, R, dir, f);
+            if (f[0] < 0.0f) wall_s(L, dir, f);
+        }
+    } else {
+        hll_s(H, L, R, dir, f);
+    }
+}
+
+template <int MODE, int LIM, bool BRACKET>
+__global__ void __launch_bounds__(HB_NT, 2) hydro_band_kernel(const __grid_constant__ CUtensorMap map, HydroArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    BandShared& sh = *reinterpret_cast<BandShared*>(smem_raw);
     const HydroConst H = A.H;
     const int w = H.w, h = H.h;
     const size_t n = (size_t)w * h;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, row = tid >> 5;
+    const int x0 = blockIdx.x * HB_TX, y0 = blockIdx.y * HB_TY;
+    const int xs = (x0 - 2) & ~3, ys = y0 - 2;  // the box's origin: x on a 16-byte boundary
     const float dt = (float)(*A.dt);
     const float half = 0.5f * dt;
     const bool grav = A.gx != nullptr;
 
-    // ---- stage: primitives of the tile grown by 2 (world cells or ghosts), raw Σ for the vacuum tests
-    for (int k = tid; k < EX * EY; k += NT) {
-        int ly = k / EX, lx = k % EX;
-        int x = x0 + lx - 2, y = y0 + ly - 2;
-        float raw = -1.0f;
+    // ---- the four planes of the staged region by one TMA box; every wait is bounded
+    if (tid == 0) {
+        tc::mbar_init(&sh.mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        tma::expect_tx(&sh.mbar, (uint32_t)sizeof(sh.raw));
+        tma::load_3d(&sh.raw[0][0][0], &map, xs, ys, 0, &sh.mbar);
+    }
+    const bool landed = tc::mbar_wait(&sh.mbar, 0, kHydroWaitPolls);
+    if (__syncthreads_or(!landed)) {
+        if (tid == 0) atomicOr(A.err, 1);
+        tc::mbar_wait(&sh.mbar, 0, kHydroWaitPolls);  // the copy still in flight lands before the CTA leaves
+        return;
+    }
+
+    // ---- primitives of the staged region: world cells, or ghosts past the edges (bounce mirrors the cells beyond
+    // with the normal velocity negated, leave copies the edge cell with it clamped outward)
+    for (int k = tid; k < HB_SY * HB_SX; k += HB_NT) {
+        const int ly = k / HB_SX, lx = k - ly * HB_SX;
+        const int x = x0 - 2 + lx, y = y0 - 2 + ly;
         Prim p;
+        float raw = -1.0f;
         if (x >= -2 && x <= w + 1 && y >= -2 && y <= h + 1) {
-            p = ghosted(H, A.U, x, y, raw);
+            const bool xo = x < 0 || x >= w, yo = y < 0 || y >= h;
+            int cx, cy;
+            if (H.edge == SR_EDGE_BOUNCE) {
+                cx = x < 0 ? -x - 1 : (x >= w ? 2 * w - 1 - x : x);
+                cy = y < 0 ? -y - 1 : (y >= h ? 2 * h - 1 - y : y);
+            } else {
+                cx = min(max(x, 0), w - 1);
+                cy = min(max(y, 0), h - 1);
+            }
+            const int bx = cx - xs, by = cy - ys;
+            const float s = sh.raw[0][by][bx];
+            p = eos_read(H, s, sh.raw[1][by][bx], sh.raw[2][by][bx], sh.raw[3][by][bx]);
+            raw = (xo || yo) ? -1.0f : s;
+            if (H.edge == SR_EDGE_BOUNCE) {
+                if (xo) p.u = -p.u;
+                if (yo) p.v = -p.v;
+            } else {
+                if (x < 0) p.u = fminf(p.u, 0.0f);
+                if (x >= w) p.u = fmaxf(p.u, 0.0f);
+                if (y < 0) p.v = fminf(p.v, 0.0f);
+                if (y >= h) p.v = fmaxf(p.v, 0.0f);
+            }
         } else {
             p.s = 1.0f; p.u = 0.0f; p.v = 0.0f; p.p = 1.0f;  // past every ghost: never reaches a kept cell
         }
         sh.P[ly][lx] = make_float4(p.s, p.u, p.v, p.p);
+        sh.Q[ly][lx] = sr_div(p.p, p.s);
         sh.S[ly][lx] = raw;
-        sh.Q[ly][lx] = p.p / p.s;
     }
     __syncthreads();
 
-    // ---- predict: the tile's cells (all four faces) and the strips around it (the face toward the tile)
-    for (int k = tid; k < NT + 2 * TY + 2 * TX; k += NT) {
-        int lx, ly, want;  // local tile coordinates of the cell, -1..TX / -1..TY
-        if (k < NT) {
-            lx = k % TX; ly = k / TX; want = 15;
-        } else if (k < NT + TY) {
-            lx = -1; ly = k - NT; want = 2;
-        } else if (k < NT + 2 * TY) {
-            lx = TX; ly = k - NT - TY; want = 1;
-        } else if (k < NT + 2 * TY + TX) {
-            lx = k - NT - 2 * TY; ly = -1; want = 8;
-        } else {
-            lx = k - NT - 2 * TY - TX; ly = TY; want = 4;
-        }
-        int sx = lx + 2, sy = ly + 2;
-        float gxv = 0.0f, gyv = 0.0f;
+    // ---- this lane's cell: slopes, the Hancock increment and the half-step centre (hydro.rs:587-614)
+    const int sx = lane + 1, sy = row + 1;  // the cell in the staged region
+    const int X = x0 - 1 + lane, Y = y0 - 1 + row;
+    const Prim c = prim_at(sh, sy, sx);
+    const Prim slx = slope<LIM, BRACKET>(prim_at(sh, sy, sx - 1), c, prim_at(sh, sy, sx + 1), sh.Q[sy][sx - 1],
+                                         sh.Q[sy][sx], sh.Q[sy][sx + 1]);
+    const Prim sly = slope<LIM, BRACKET>(prim_at(sh, sy - 1, sx), c, prim_at(sh, sy + 1, sx), sh.Q[sy - 1][sx],
+                                         sh.Q[sy][sx], sh.Q[sy + 1][sx]);
+    float gxv = 0.0f, gyv = 0.0f;
+    if (grav) {  // a ghost takes its edge cell's g
+        const size_t gi = (size_t)min(max(Y, 0), h - 1) * w + min(max(X, 0), w - 1);
+        gxv = A.gx[gi];
+        gyv = A.gy[gi];
+    }
+    float delta[4];
+    {
+        float a[4], b[4], dxs[4];
+        face_flux(H, c, slx, -0.5f, 0, a);
+        face_flux(H, c, slx, 0.5f, 0, b);
+#pragma unroll
+        for (int k = 0; k < 4; k++) dxs[k] = a[k] - b[k];
+        face_flux(H, c, sly, -0.5f, 1, a);
+        face_flux(H, c, sly, 0.5f, 1, b);
+#pragma unroll
+        for (int k = 0; k < 4; k++) delta[k] = half * (dxs[k] + (a[k] - b[k]));
+    }
+    {
+        float m1 = c.s * c.u + delta[1], m2 = c.s * c.v + delta[2];
         if (grav) {
-            int cx = min(max(x0 + lx, 0), w - 1), cy = min(max(y0 + ly, 0), h - 1);  // a ghost takes its edge cell's g
-            size_t i = (size_t)cy * w + cx;
-            gxv = A.gx[i];
-            gyv = A.gy[i];
+            m1 += half * c.s * gxv;
+            m2 += half * c.s * gyv;
         }
-        Face f[4];
-        float mid[3];
-        const float q[5] = {sh.Q[sy][sx - 1], sh.Q[sy][sx], sh.Q[sy][sx + 1], sh.Q[sy - 1][sx], sh.Q[sy + 1][sx]};
-        predict(H, P_at(sh, sy, sx - 1), P_at(sh, sy, sx), P_at(sh, sy, sx + 1), P_at(sh, sy - 1, sx),
-                P_at(sh, sy + 1, sx), q, half, grav, gxv, gyv, want, f, mid);
-        if (k < NT) {
+        sh.M[0][row][lane] = c.s + delta[0];
+        sh.M[1][row][lane] = m1;
+        sh.M[2][row][lane] = m2;
+    }
+
+    // ---- x faces: this lane's x+ face against the next lane's x- face; the left face's flux from the lane before
+    float fr[4], fl[4];
+    {
+        const FaceS R = shfl_face_down(face_state(H, c, slx, -0.5f, delta, half, grav, gxv, gyv));
+        const FaceS L = face_state(H, c, slx, 0.5f, delta, half, grav, gxv, gyv);
+        face_flux_at(H, L, R, 0, X + 1, w, Y >= 0 && Y < h, fr);
 #pragma unroll
-            for (int q = 0; q < 4; q++) sh.F[q][ly][lx] = f[q];
-        } else if (lx == -1) {
-            sh.FL[ly] = f[1];
-        } else if (lx == TX) {
-            sh.FR[ly] = f[0];
-        } else if (ly == -1) {
-            sh.FT[lx] = f[3];
-        } else {
-            sh.FB[lx] = f[2];
-        }
-        sh.M[ly + 1][lx + 1][0] = mid[0];
-        sh.M[ly + 1][lx + 1][1] = mid[1];
-        sh.M[ly + 1][lx + 1][2] = mid[2];
+        for (int k = 0; k < 4; k++) fl[k] = __shfl_up_sync(0xffffffffu, fr[k], 1);
+    }
+    // ---- y faces: the row above's y+ faces against this row's y- faces, through shared memory
+    {
+        const FaceS T = face_state(H, c, sly, 0.5f, delta, half, grav, gxv, gyv);
+        sh.YF[0][row][lane] = T.U0;
+        sh.YF[1][row][lane] = T.U1;
+        sh.YF[2][row][lane] = T.U2;
+        sh.YF[3][row][lane] = T.U3;
+        sh.YF[4][row][lane] = T.u;
+        sh.YF[5][row][lane] = T.v;
+        sh.YF[6][row][lane] = T.P;
+    }
+    const FaceS B = face_state(H, c, sly, -0.5f, delta, half, grav, gxv, gyv);
+    __syncthreads();
+    if (row >= 1) {
+        FaceS L;
+        L.U0 = sh.YF[0][row - 1][lane];
+        L.U1 = sh.YF[1][row - 1][lane];
+        L.U2 = sh.YF[2][row - 1][lane];
+        L.U3 = sh.YF[3][row - 1][lane];
+        L.u = sh.YF[4][row - 1][lane];
+        L.v = sh.YF[5][row - 1][lane];
+        L.P = sh.YF[6][row - 1][lane];
+        float ft[4];
+        face_flux_at(H, L, B, 1, Y, h, X >= 0 && X < w, ft);
+#pragma unroll
+        for (int k = 0; k < 4; k++) sh.FY[k][row][lane] = ft[k];
     }
     __syncthreads();
 
-    // ---- fluxes: x faces then y faces; the world's edge faces by the edge mode (hydro.rs:564-582, 744-775)
-    for (int k = tid; k < (TX + 1) * TY + TX * (TY + 1); k += NT) {
-        float f[4];
-        if (k < (TX + 1) * TY) {
-            int i = k % (TX + 1), j = k / (TX + 1);
-            int X = x0 + i;
-            const Face& L = i == 0 ? sh.FL[j] : sh.F[1][j][i - 1];
-            const Face& R = i == TX ? sh.FR[j] : sh.F[0][j][i];
-            if (X > w || y0 + j >= h) {
-                f[0] = f[1] = f[2] = f[3] = 0.0f;
-            } else if (X == 0) {
-                if (H.edge == SR_EDGE_BOUNCE) {
-                    wall(R, 0, f);
-                } else {
-                    hll(H, L, R, 0, f);
-                    if (f[0] > 0.0f) wall(R, 0, f);
-                }
-            } else if (X == w) {
-                if (H.edge == SR_EDGE_BOUNCE) {
-                    wall(L, 0, f);
-                } else {
-                    hll(H, L, R, 0, f);
-                    if (f[0] < 0.0f) wall(L, 0, f);
-                }
-            } else {
-                hll(H, L, R, 0, f);
-            }
+    // ---- epilogue: the tile's cells
+    const bool inside = lane >= 1 && lane <= HB_TX && row >= 1 && row <= HB_TY && X < w && Y < h;
+    const size_t i = inside ? (size_t)Y * w + X : 0;
+    float fu[4], fd[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) sh.FX[j][i][q] = f[q];
-        } else {
-            int kk = k - (TX + 1) * TY;
-            int i = kk % TX, j = kk / TX;
-            int Y = y0 + j;
-            const Face& L = j == 0 ? sh.FT[i] : sh.F[3][j - 1][i];
-            const Face& R = j == TY ? sh.FB[i] : sh.F[2][j][i];
-            if (Y > h || x0 + i >= w) {
-                f[0] = f[1] = f[2] = f[3] = 0.0f;
-            } else if (Y == 0) {
-                if (H.edge == SR_EDGE_BOUNCE) {
-                    wall(R, 1, f);
-                } else {
-                    hll(H, L, R, 1, f);
-                    if (f[0] > 0.0f) wall(R, 1, f);
-                }
-            } else if (Y == h) {
-                if (H.edge == SR_EDGE_BOUNCE) {
-                    wall(L, 1, f);
-                } else {
-                    hll(H, L, R, 1, f);
-                    if (f[0] < 0.0f) wall(L, 1, f);
-                }
-            } else {
-                hll(H, L, R, 1, f);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; q++) sh.FY[j][i][q] = f[q];
-        }
+    for (int k = 0; k < 4; k++) {
+        fu[k] = row >= 1 ? sh.FY[k][row][lane] : 0.0f;
+        fd[k] = row + 1 < HB_W ? sh.FY[k][row + 1][lane] : 0.0f;
     }
-    __syncthreads();
-
-    // ---- epilogue: one thread per tile cell
-    const int lx = tid % TX, ly = tid / TX;
-    const int X = x0 + lx, Y = y0 + ly;
-    const bool inside = X < w && Y < h;
-    const size_t i = (size_t)Y * w + X;
     // a cell with no gas around it stays empty (hydro.rs:733-742); out-of-world neighbours read as vacuum
-    const int sx = lx + 2, sy = ly + 2;
     const float sv = H.sigma_vac;
     const bool vac = sh.S[sy][sx] < sv;
     const bool empty = vac && sh.S[sy][sx - 1] < sv && sh.S[sy][sx + 1] < sv && sh.S[sy - 1][sx] < sv &&
                        sh.S[sy + 1][sx] < sv;
-    const float* fl = sh.FX[ly][lx];
-    const float* fr = sh.FX[ly][lx + 1];
-    const float* fu = sh.FY[ly][lx];
-    const float* fd = sh.FY[ly + 1][lx];
 
     if (MODE == kHydroSource) {
         if (!inside) return;
@@ -373,8 +401,8 @@ __global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 
         if (empty) {
             s = 0.0f;
         } else {
-            float start = vac ? sh.P[sy][sx].x : sh.S[sy][sx];
-            float div = (fr[0] - fl[0]) + (fd[0] - fu[0]);
+            const float start = vac ? sh.P[sy][sx].x : sh.S[sy][sx];
+            const float div = (fr[0] - fl[0]) + (fd[0] - fu[0]);
             s = 0.5f * (sh.S[sy][sx] + (start - dt * div));
         }
         A.src[i] = s >= sv ? s : 0.0f;
@@ -386,20 +414,19 @@ __global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 
     int best_i = -1;
     double esc[4] = {0.0, 0.0, 0.0, 0.0};
     if (inside) {
+        const int bx = X - xs, by = Y - ys;
         float u[4];
-        if (empty) {
-            u[0] = A.U[i]; u[1] = A.U[n + i]; u[2] = A.U[2 * n + i]; u[3] = A.U[3 * n + i];
+        if (empty || !vac) {
+            u[0] = sh.raw[0][by][bx]; u[1] = sh.raw[1][by][bx]; u[2] = sh.raw[2][by][bx]; u[3] = sh.raw[3][by][bx];
         } else {
-            if (vac) {
-                eos_cons(H, P_at(sh, sy, sx), u);
-            } else {
-                u[0] = A.U[i]; u[1] = A.U[n + i]; u[2] = A.U[2 * n + i]; u[3] = A.U[3 * n + i];
-            }
+            eos_cons(H, c, u);
+        }
+        if (!empty) {
 #pragma unroll
             for (int q = 0; q < 4; q++) u[q] -= dt * ((fr[q] - fl[q]) + (fd[q] - fu[q]));
             if (MODE == kHydroUpdateGrav) {
-                const float* m = sh.M[ly + 1][lx + 1];
-                float src = A.src[i];
+                const float m[3] = {sh.M[0][row][lane], sh.M[1][row][lane], sh.M[2][row][lane]};
+                const float src = A.src[i];
                 float kick[2] = {dt * src * A.gxm[i], dt * src * A.gym[i]};
                 kick_acc[0] = (double)kick[0];
                 kick_acc[1] = (double)kick[1];
@@ -407,13 +434,30 @@ __global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 
                     best = src;
                     best_i = (int)i;
                 }
-                float p = A.phim[i];
+                const float p = A.phim[i];
                 float pr = p, pl = p, pd = p, pu = p;
-                const float *mr = m, *ml = m, *md = m, *mu = m;
-                if (X + 1 < w) { pr = A.phim[i + 1]; mr = sh.M[ly + 1][lx + 2]; }
-                if (X > 0) { pl = A.phim[i - 1]; ml = sh.M[ly + 1][lx]; }
-                if (Y + 1 < h) { pd = A.phim[i + w]; md = sh.M[ly + 2][lx + 1]; }
-                if (Y > 0) { pu = A.phim[i - w]; mu = sh.M[ly][lx + 1]; }
+                float mr[3] = {m[0], m[1], m[2]}, ml[3] = {m[0], m[1], m[2]}, md[3] = {m[0], m[1], m[2]},
+                      mu[3] = {m[0], m[1], m[2]};
+                if (X + 1 < w) {
+                    pr = A.phim[i + 1];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) mr[q] = sh.M[q][row][lane + 1];
+                }
+                if (X > 0) {
+                    pl = A.phim[i - 1];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) ml[q] = sh.M[q][row][lane - 1];
+                }
+                if (Y + 1 < h) {
+                    pd = A.phim[i + w];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) md[q] = sh.M[q][row + 1][lane];
+                }
+                if (Y > 0) {
+                    pu = A.phim[i - w];
+#pragma unroll
+                    for (int q = 0; q < 3; q++) mu[q] = sh.M[q][row - 1][lane];
+                }
                 float r[3], l[3], dn[3], up[3];
                 face_work(fr[0], m[0], mr[0], m[1], mr[1], p - pr, dt, r);
                 face_work(fl[0], ml[0], m[0], ml[1], m[1], pl - p, dt, l);
@@ -426,7 +470,7 @@ __global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 
                 u[3] += r[1] + l[2] + dn[1] + up[2];
             }
             // escaped (hydro.rs:948-973): the boundary faces' fluxes as the cell took them
-            float phi_edge = MODE == kHydroUpdateGrav ? A.phim[i] : 0.0f;
+            const float phi_edge = MODE == kHydroUpdateGrav ? A.phim[i] : 0.0f;
             if (X == 0) { for (int q = 0; q < 4; q++) esc[q] -= (double)(dt * fl[q]); esc[3] -= (double)(dt * fl[0] * phi_edge); }
             if (X + 1 == w) { for (int q = 0; q < 4; q++) esc[q] += (double)(dt * fr[q]); esc[3] += (double)(dt * fr[0] * phi_edge); }
             if (Y == 0) { for (int q = 0; q < 4; q++) esc[q] -= (double)(dt * fu[q]); esc[3] -= (double)(dt * fu[0] * phi_edge); }
@@ -439,44 +483,45 @@ __global__ void __launch_bounds__(NT, 3) hydro_tile_kernel(HydroArgs A) {  // 3 
     }
 
     // ---- per-CTA partials in a fixed order: Σ kicks (FP64), the densest cell (max src, lowest index), Σ escaped
-    __shared__ double red_d[6][NT / 32];
-    __shared__ float red_best[NT / 32];
-    __shared__ int red_idx[NT / 32];
-    const int lane = tid & 31, warp = tid >> 5;
+    // a warp whose lanes hold no term skips its tree (interior rows hold no escaped flux; only the gravity pass kicks)
     double vals[6] = {kick_acc[0], kick_acc[1], esc[0], esc[1], esc[2], esc[3]};
 #pragma unroll
     for (int q = 0; q < 6; q++) {
         double v = vals[q];
+        if (__any_sync(0xffffffffu, v != 0.0)) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) red_d[q][warp] = v;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        }
+        if (lane == 0) sh.red_d[q][row] = v;
     }
+    if (__any_sync(0xffffffffu, best_i >= 0)) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        float ob = __shfl_down_sync(0xffffffffu, best, o);
-        int oi = __shfl_down_sync(0xffffffffu, best_i, o);
-        if (oi >= 0 && (best_i < 0 || ob > best || (ob == best && oi < best_i))) {
-            best = ob;
-            best_i = oi;
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ob = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, best_i, o);
+            if (oi >= 0 && (best_i < 0 || ob > best || (ob == best && oi < best_i))) {
+                best = ob;
+                best_i = oi;
+            }
         }
     }
     if (lane == 0) {
-        red_best[warp] = best;
-        red_idx[warp] = best_i;
+        sh.red_best[row] = best;
+        sh.red_idx[row] = best_i;
     }
     __syncthreads();
     if (tid == 0) {
         const int b = blockIdx.y * gridDim.x + blockIdx.x;
         for (int q = 0; q < 6; q++) {
             double t = 0.0;
-            for (int k = 0; k < NT / 32; k++) t += red_d[q][k];
+            for (int k = 0; k < HB_W; k++) t += sh.red_d[q][k];
             A.part_d[(size_t)b * 6 + q] = t;
         }
         float bb = 0.0f;
         int bi = -1;
-        for (int k = 0; k < NT / 32; k++) {
-            int oi = red_idx[k];
-            float ob = red_best[k];
+        for (int k = 0; k < HB_W; k++) {
+            const int oi = sh.red_idx[k];
+            const float ob = sh.red_best[k];
             if (oi >= 0 && (bi < 0 || ob > bb || (ob == bb && oi < bi))) {
                 bb = ob;
                 bi = oi;
@@ -540,31 +585,59 @@ __global__ void hydro_finalize_kernel(HydroArgs A, int nblocks, int take_back) {
 
 }  // namespace
 
-size_t hydro_smem_bytes() { return sizeof(Shared); }
 
-int hydro_blocks(int w, int h) { return (int)(div_up(w, TX) * div_up(h, TY)); }
+size_t hydro_smem_bytes() { return sizeof(BandShared); }
+
+int hydro_blocks(int w, int h) { return (int)(div_up(w, HB_TX) * div_up(h, HB_TY)); }
+
+void tma_encode_planes(CUtensorMap* map, const float* base, int w, int h, int planes, int bx, int by) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SR_CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        SR_REQUIRE(q == cudaDriverEntryPointSuccess && fn, "the driver has no cuTensorMapEncodeTiled");
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    SR_REQUIRE(w % 4 == 0 && ((uintptr_t)base & 15) == 0, "a TMA plane needs 16-byte rows and a 16-byte base");
+    const cuuint64_t dims[3] = {(cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)planes};
+    const cuuint64_t strides[2] = {(cuuint64_t)w * sizeof(float), (cuuint64_t)w * h * sizeof(float)};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)planes};
+    const cuuint32_t unit[3] = {1, 1, 1};
+    const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box,
+                              unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw SrError{SR_E_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r)};
+}
+
+template <int MODE, int LIM, bool BRACKET>
+void hydro_launch_t(const CUtensorMap& map, const HydroArgs& A, cudaStream_t s) {
+    static bool attr = false;  // the attribute of this instance, once per process
+    if (!attr) {
+        SR_CUDA_TRY(cudaFuncSetAttribute(hydro_band_kernel<MODE, LIM, BRACKET>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BandShared)));
+        attr = true;
+    }
+    const dim3 grid(div_up(A.H.w, HB_TX), div_up(A.H.h, HB_TY));
+    hydro_band_kernel<MODE, LIM, BRACKET><<<grid, HB_NT, sizeof(BandShared), s>>>(map, A);
+    sr_note_launch();
+}
+
+template <int MODE>
+void hydro_launch_m(const CUtensorMap& map, const HydroArgs& A, cudaStream_t s) {
+    const bool mc = A.H.limiter != SR_LIMITER_MINMOD, br = A.H.bracket != 0;
+    if (mc && br) hydro_launch_t<MODE, SR_LIMITER_MC, true>(map, A, s);
+    else if (mc) hydro_launch_t<MODE, SR_LIMITER_MC, false>(map, A, s);
+    else if (br) hydro_launch_t<MODE, SR_LIMITER_MINMOD, true>(map, A, s);
+    else hydro_launch_t<MODE, SR_LIMITER_MINMOD, false>(map, A, s);
+}
 
 void hydro_launch(int mode, const HydroArgs& A, cudaStream_t s) {
-    dim3 grid(div_up(A.H.w, TX), div_up(A.H.h, TY));
-    size_t smem = sizeof(Shared);
-    switch (mode) {
-        case kHydroUpdate:
-            cudaFuncSetAttribute(hydro_tile_kernel<kHydroUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            hydro_tile_kernel<kHydroUpdate><<<grid, NT, smem, s>>>(A);
-    sr_note_launch();
-            break;
-        case kHydroSource:
-            cudaFuncSetAttribute(hydro_tile_kernel<kHydroSource>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            hydro_tile_kernel<kHydroSource><<<grid, NT, smem, s>>>(A);
-    sr_note_launch();
-            break;
-        default:
-            cudaFuncSetAttribute(hydro_tile_kernel<kHydroUpdateGrav>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-            hydro_tile_kernel<kHydroUpdateGrav><<<grid, NT, smem, s>>>(A);
-    sr_note_launch();
-            break;
-    }
+    CUtensorMap map;
+    tma_encode_planes(&map, A.U, A.H.w, A.H.h, 4, HB_BX, HB_BY);
+    if (mode == kHydroUpdate) hydro_launch_m<kHydroUpdate>(map, A, s);
+    else if (mode == kHydroSource) hydro_launch_m<kHydroSource>(map, A, s);
+    else hydro_launch_m<kHydroUpdateGrav>(map, A, s);
 }
 
 void hydro_finalize_launch(const HydroArgs& A, int take_back, cudaStream_t s) {

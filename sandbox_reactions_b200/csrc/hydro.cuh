@@ -3,7 +3,6 @@
 
 #include "common.cuh"
 
-constexpr int kHydroTileX = 32, kHydroTileY = 8;
 enum { kHydroUpdate = 0, kHydroSource = 1, kHydroUpdateGrav = 2 };
 
 // The Δt record kept on the device (crates/sr-engine/src/step/dt.rs:51-61): steps never wait on the host for it.
@@ -33,6 +32,7 @@ struct HydroArgs {
     float* part_best;          // per-CTA densest Σ_src,mid and its cell
     int* part_idx;
     double* report;            // [kick x, kick y, densest, escaped Σ, Σu, Σv, E]
+    int* err;                  // set to 1 when a bounded wait of the kernel gave up (its TMA box never landed)
 };
 
 size_t hydro_smem_bytes();
