@@ -240,6 +240,7 @@ static void run_steps(sr_ctx* c, uint32_t steps) {
     }
     if (c->timing && steps) {
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (c->heat) heat_account_launches(c->heat, c->stream);
         sr_cost& t = c->cost;
         memset(&t, 0, sizeof t);
         t.steps = steps;
@@ -437,6 +438,7 @@ sr_status sr_read_heat(sr_ctx* c, sr_heat_report* out) {
     return guarded(c, [&] {
         SR_REQUIRE(out, "sr_read_heat: null report");
         SR_REQUIRE(c->cfg.heat, "sr_read_heat: the context runs no heat pass");
+        heat_report(c->heat, c->stream, &c->heat_report);
         *out = c->heat_report;
     });
 }

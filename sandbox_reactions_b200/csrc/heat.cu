@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
 #include <vector>
 
 #include "heat.cuh"
@@ -20,10 +21,18 @@
 namespace {
 
 constexpr int RED_THREADS = 256;
+constexpr double kFirstPassTol = 0.1;  // the first Newton pass's relative residual (and the loosest any pass asks)
+constexpr double kTrustedPassTol = 1e-5;  // passes this loose end on their FP32 solve's own test
+constexpr int kMaxRefinements = 16;    // FP64 refinement sweeps per Newton pass
 constexpr int MAX_PART = 1184;    // most CTAs of a grid-stride heat kernel: one wave (148 SMs x 8), few partials to sum
 constexpr int PART_CAP = 16384;   // partials per reduced value (the level-0 smoother's CTAs included)
+// Device scalars. The kernels read Δt, the refinement's scale, δ and the PCG round's state from here (never from
+// launch arguments), so a captured graph of the implicit step replays for any step. The fused MG/Jacobi rounds keep
+// <r, z> of this round (S_RZC), of the last (S_RZP) and from the next preconditioner application (S_RZN), and which
+// direction buffer is current (S_PAR); the flexible (learned) rounds use S_RZ0/S_RZ1.
 enum Slot { S_HEAT0, S_NGAS, S_DT, S_RR, S_BB, S_GAM, S_HM, S_MOVED, S_VIOL, S_UB, S_TB, S_R32, S_PQ, S_RRI, S_RZ0, S_RZ1,
-            S_ZRO, S_MGRZ, S_BETA, S_RAD, S_GAIN, S_HELD, S_COUNT };
+            S_ZRO, S_MGRZ, S_BETA, S_RAD, S_GAIN, S_HELD, S_RZC, S_RZP, S_RZN, S_PAR, S_SCALE, S_ISCALE, S_DELTA,
+            S_COUNT };
 
 // Where a kernel's grid sum goes: the partials buffer, the ticket counter and the device scalar(s).
 struct Red {
@@ -202,13 +211,14 @@ __global__ void heat_ksum_kernel(HeatConst K, const uint8_t* __restrict__ gas, c
 // ---- a Newton pass's system at the iterate (heat.rs:476-489), kept as its mass term c = c_i + Σ_vac D_f (the
 // diagonal less the couplings to gas neighbours, f64; FP32 copy as level 0's c) so that A x = c x + Σ D (x_i - x_j)
 // is evaluated without cancellation; partials of the two measures' bounds, Σ c_i u² and Σ (C/Δt) T² (heat.rs:480-487).
-__global__ void heat_system_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+__global__ void heat_system_kernel(HeatConst K, const double* __restrict__ scal, const uint8_t* __restrict__ gas,
                                    const double* __restrict__ C, const double* __restrict__ t,
                                    const double* __restrict__ u, const double* __restrict__ t0,
                                    const double* __restrict__ kvac, double* c64, double* rhs, float* c0, double* x,
                                    Red R) {
     const size_t n = (size_t)K.w * K.h;
     const double u_vac = u_of(K, K.t_floor);
+    const double dt = scal[S_DT];
     double ub = 0.0, tb = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) {
@@ -237,13 +247,14 @@ __global__ void heat_system_kernel(HeatConst K, double dt, const uint8_t* __rest
 // the flags select afterwards), so a thread keeps several DRAM requests in flight.
 constexpr int ILP = 4;
 
-__global__ void heat_residual64_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+__global__ void heat_residual64_kernel(HeatConst K, const double* __restrict__ scal, const uint8_t* __restrict__ gas,
                                        const double* __restrict__ c64, const double* __restrict__ rhs,
                                        const double* __restrict__ kx, const double* __restrict__ ky,
                                        const double* __restrict__ C, const double* __restrict__ t,
                                        const double* __restrict__ x, double* __restrict__ r, Red R) {
     const int w = K.w, h = K.h;
     const size_t n = (size_t)w * h, stride = (size_t)gridDim.x * blockDim.x;
+    const double dt = scal[S_DT];
     double rr = 0.0, bb = 0.0, gg = 0.0, hh = 0.0;
     for (size_t base = (size_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += 2 * stride) {
 #pragma unroll
@@ -293,8 +304,9 @@ __global__ void heat_residual64_kernel(HeatConst K, double dt, const uint8_t* __
     grid_sum_last<4>(v, R.part, R.counter, R.out);
 }
 
-__global__ void scale_kernel(size_t n, const double* __restrict__ r64, double inv_scale, float* r32, float* e32,
-                             Red R) {
+__global__ void scale_kernel(size_t n, const double* __restrict__ r64, const double* __restrict__ scal, float* r32,
+                             float* e32, Red R) {
+    const double inv_scale = scal[S_ISCALE];
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const float v = (float)(r64[i] * inv_scale);
@@ -405,12 +417,15 @@ __global__ void pcg_direction_kernel(size_t n, const double* __restrict__ scal, 
 // The fused round head of (non-flexible) PCG: the search direction p_new = z + β p (β = <r,z>_cur / <r,z>_prev, or
 // p_new = z while the S_BETA flag is 0: the first round) and q = A p_new in difference form, with partials of
 // <p_new, q>; the last CTA sets the flag. Four consecutive cells of a row per thread with 16-byte loads (W is a
-// multiple of 8); the neighbours' p_new are formed from their z and old p, so p_new goes to its own buffer.
-__global__ void spmv_dir_kernel(MgLevel L, const double* __restrict__ scal, int cur, int prev,
-                                const float* __restrict__ z, const float* __restrict__ p, float* __restrict__ pnew,
-                                float* __restrict__ q, Red R, double* beta_flag) {
+// multiple of 8); the neighbours' p_new are formed from their z and old p, so p_new goes to the other of the two
+// direction buffers (S_PAR says which holds the old one).
+__global__ void spmv_dir_kernel(MgLevel L, const double* __restrict__ scal, const float* __restrict__ z, float* pa,
+                                float* pb, float* __restrict__ q, Red R, double* beta_flag) {
     const bool first = scal[S_BETA] == 0.0;  // p = z: the old direction is not read (it may hold anything)
-    const float beta = first ? 0.0f : (float)(scal[cur] / scal[prev]);
+    const float beta = first ? 0.0f : (float)(scal[S_RZC] / scal[S_RZP]);
+    const bool par = scal[S_PAR] != 0.0;
+    const float* __restrict__ p = par ? pb : pa;
+    float* __restrict__ pnew = par ? pa : pb;
     const int w = L.w, h = L.h;
     const size_t n4 = (size_t)w * h / 4, stride = (size_t)gridDim.x * blockDim.x;
     double acc = 0.0;
@@ -457,10 +472,11 @@ __global__ void spmv_dir_kernel(MgLevel L, const double* __restrict__ scal, int 
     if (grid_sum_last1(acc, R.part, R.counter, R.out) && threadIdx.x == 0 && beta_flag) *beta_flag = 1.0;
 }
 
-// e += α p, r -= α q with 16-byte accesses (four cells per thread); partials of <r, r>.
-__global__ void pcg_update4_kernel(size_t n, const double* __restrict__ scal, int rz_slot, const float* __restrict__ p,
+// e += α p, r -= α q with 16-byte accesses (four cells per thread), p the round's new direction; partials of <r, r>.
+__global__ void pcg_update4_kernel(size_t n, const double* __restrict__ scal, const float* pa, const float* pb,
                                    const float* __restrict__ q, float* __restrict__ e, float* __restrict__ r, Red R) {
-    const float alpha = (float)(scal[rz_slot] / scal[S_PQ]);
+    const float alpha = (float)(scal[S_RZC] / scal[S_PQ]);
+    const float* __restrict__ p = scal[S_PAR] != 0.0 ? pa : pb;
     const size_t n4 = n / 4, stride = (size_t)gridDim.x * blockDim.x;
     double acc = 0.0;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += stride) {
@@ -556,7 +572,8 @@ __global__ void add_dot_kernel(size_t n, const float* __restrict__ r, const floa
 }
 
 __global__ void correction_kernel(size_t n, const uint8_t* __restrict__ gas, const float* __restrict__ e,
-                                  double scale, double* x) {
+                                  const double* __restrict__ scal, double* x) {
+    const double scale = scal[S_SCALE];
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         if (gas[i]) x[i] += scale * (double)e[i];
 }
@@ -565,12 +582,14 @@ __global__ void correction_kernel(size_t n, const uint8_t* __restrict__ gas, con
 // (as heat_system_kernel builds it) in one sweep over the cells; partials of Σ C|ΔT|, the cells moved by more than
 // newton_cell of their T, Σ c_i u² and Σ (C/Δt) T² (four consecutive slots from S_MOVED). When the passes end here
 // the system goes unused.
-__global__ void newton_system_kernel(HeatConst K, double cell_tol, double dt, const uint8_t* __restrict__ gas,
+__global__ void newton_system_kernel(HeatConst K, double cell_tol, const double* __restrict__ scal,
+                                     const uint8_t* __restrict__ gas,
                                      const double* __restrict__ C, const double* __restrict__ t0,
                                      const double* __restrict__ kvac, double* t, double* u, double* x, double* c64,
                                      double* rhs, float* c0, Red R) {
     const size_t n = (size_t)K.w * K.h, stride = (size_t)gridDim.x * blockDim.x;
     const double u_vac = u_of(K, K.t_floor);
+    const double dt = scal[S_DT];
     double moved = 0.0, viol = 0.0, ub = 0.0, tb = 0.0;
     // two cells a grid stride apart per iteration, all loads issued before the arithmetic
     for (size_t base = (size_t)blockIdx.x * blockDim.x + threadIdx.x; base < n; base += 2 * stride) {
@@ -657,12 +676,13 @@ __global__ void heat_flux_kernel(HeatConst K, const uint8_t* __restrict__ gas, c
 }
 
 // The commit's sums (heat.rs:521-531): radiated, gained and held.
-__global__ void commit_sums_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+__global__ void commit_sums_kernel(HeatConst K, const double* __restrict__ scal, const uint8_t* __restrict__ gas,
                                    const double* __restrict__ C, const double* __restrict__ t,
                                    const double* __restrict__ t0, const double* __restrict__ u,
                                    const double* __restrict__ kvac, Red R) {
     const size_t n = (size_t)K.w * K.h;
     const double u_vac = u_of(K, K.t_floor);
+    const double dt = scal[S_DT];
     double rad = 0.0, gain = 0.0, held = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) continue;
@@ -676,10 +696,11 @@ __global__ void commit_sums_kernel(HeatConst K, double dt, const uint8_t* __rest
 
 // E_i += C_i ((1 + δ) T_i - T_i⁰) (heat.rs:532-535), and the cell's rate (T - T⁰)/Δt kept for the next step's first
 // iterate (heat.wgsl:1139-1155).
-__global__ void commit_apply_kernel(HeatConst K, double delta, double dt, const uint8_t* __restrict__ gas,
+__global__ void commit_apply_kernel(HeatConst K, const double* __restrict__ scal, const uint8_t* __restrict__ gas,
                                     const double* __restrict__ C, const double* __restrict__ t,
                                     const double* __restrict__ t0, float* U, double* rate) {
     const size_t n = (size_t)K.w * K.h;
+    const double delta = scal[S_DELTA], dt = scal[S_DT];
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (gas[i]) U[3 * n + i] = (float)((double)U[3 * n + i] + C[i] * ((1.0 + delta) * t[i] - t0[i]));
         rate[i] = gas[i] ? (t[i] - t0[i]) / dt : 0.0;
@@ -688,9 +709,10 @@ __global__ void commit_apply_kernel(HeatConst K, double delta, double dt, const 
 
 // The first iterate on the V-cycle (heat.wgsl:710-722): T⁰ + the last step's rate × Δt, T⁰ where that is off by more
 // than a factor 2 or not finite, floored at T_floor.
-__global__ void warm_start_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+__global__ void warm_start_kernel(HeatConst K, const double* __restrict__ scal, const uint8_t* __restrict__ gas,
                                   const double* __restrict__ t0, const double* __restrict__ rate, double* t, double* u) {
     const size_t n = (size_t)K.w * K.h;
+    const double dt = scal[S_DT];
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) continue;
         double tg = t0[i] + rate[i] * dt;
@@ -702,13 +724,14 @@ __global__ void warm_start_kernel(HeatConst K, double dt, const uint8_t* __restr
 }
 
 // Past the ceiling (heat.rs:545-564): each gas cell's outflow scaled to the heat it holds above its floor.
-__global__ void limited_scale_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+__global__ void limited_scale_kernel(HeatConst K, const double* __restrict__ scal, const uint8_t* __restrict__ gas,
                                      const double* __restrict__ kx, const double* __restrict__ ky,
                                      const double* __restrict__ u, const double* __restrict__ C,
                                      const double* __restrict__ t0, double* scale) {
     const int w = K.w, h = K.h;
     const size_t n = (size_t)w * h;
     const double u_vac = u_of(K, K.t_floor);
+    const double dt = scal[S_DT];
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) {
             scale[i] = 1.0;
@@ -730,13 +753,14 @@ __global__ void limited_scale_kernel(HeatConst K, double dt, const uint8_t* __re
 }
 
 // E -= Δt Σ_f F_f with every face's F at the scale of the cell it leaves (heat.rs:565-592); partials of radiated.
-__global__ void limited_apply_kernel(HeatConst K, double dt, const uint8_t* __restrict__ gas,
+__global__ void limited_apply_kernel(HeatConst K, const double* __restrict__ scal, const uint8_t* __restrict__ gas,
                                      const double* __restrict__ kx, const double* __restrict__ ky,
                                      const double* __restrict__ u, const double* __restrict__ scale, float* U,
                                      Red R) {
     const int w = K.w, h = K.h;
     const size_t n = (size_t)w * h;
     const double u_vac = u_of(K, K.t_floor);
+    const double dt = scal[S_DT];
     double rad = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) continue;
@@ -763,6 +787,212 @@ __global__ void limited_apply_kernel(HeatConst K, double dt, const uint8_t* __re
         U[3 * n + i] = (float)((double)U[3 * n + i] - dt * (((out[0] + out[1]) + out[2]) + out[3]));
     }
     grid_sum_last1(rad, R.part, R.counter, R.out);
+}
+
+__global__ void zero_kernel(double* a, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) a[i] = 0.0;
+}
+
+// One device scalar set by the host's launch (a value captured at launch time, so no staging buffer is reused).
+__global__ void set_scalar_kernel(double* scal, int slot, double value) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) scal[slot] = value;
+}
+
+// A fused PCG solve's start, after its first preconditioner application: that <r, z> is the current one, the first
+// direction is z, the direction buffers start at pa.
+__global__ void pcg_start_kernel(double* scal) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    scal[S_RZC] = scal[S_RZN];
+    scal[S_BETA] = 0.0;
+    scal[S_PAR] = 0.0;
+}
+
+// A fused PCG round's end: the new <r, z> becomes the current one and the new direction buffer the old.
+__global__ void pcg_rotate_kernel(double* scal) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    scal[S_RZP] = scal[S_RZC];
+    scal[S_RZC] = scal[S_RZN];
+    scal[S_PAR] = scal[S_PAR] != 0.0 ? 0.0 : 1.0;
+}
+
+// ---- the implicit step under device control (MG and Jacobi preconditioners)
+//
+// The host-driven step (heat_step's Newton loop, solve_pass's FP64 refinement, inner_pcg's rounds) decides from
+// read-back scalars. Here the same decisions are taken by one-thread controller kernels that run between the step's
+// kernels inside one captured CUDA graph and steer its conditional nodes: an IF around the step (no gas, pinned
+// temperature or Δt <= 0 leave only the fluxes), a WHILE over the Newton passes, a WHILE over a pass's refinements, an
+// IF around each inner solve, a WHILE over its PCG rounds (the residual tested after every round: no host round trip,
+// no predicted cadence), an IF around the next pass's coarsening, and IFs choosing the commit. No launch argument
+// changes from step to step: Δt, the scale, δ and the round state live in the device scalars.
+struct HeatCtl {
+    // configuration (host-written)
+    double tol, nheat, ncell, inner_floor;
+    int max_passes, max_rounds, pin;
+    // the step
+    double heat0, n_gas;
+    int passes, rounds, refinements, converged, ok, skipped;
+    double pass_tol, moved_prev, rel;
+    // the pass's refinement and its inner solve
+    int ref, reached, it, max_it;
+    double prev, eta, rr0;
+    // the commit
+    double delta, radiated;
+    // how often each body ran since the host last counted (for the launch count)
+    unsigned long long runs[10];
+};
+enum CtlBody { B_MAIN, B_SKIP, B_PASS, B_REFINE, B_INNER, B_ROUND, B_NSYS, B_COARSEN, B_CONV, B_LIM, B_COUNT };
+
+struct CtlHandles {
+    cudaGraphConditionalHandle h[B_COUNT];
+};
+
+enum CtlPhase { C_BEGIN, C_NEWTON_BEGIN, C_PASS_BEGIN, C_REFINE, C_INNER_BEGIN, C_ROUND, C_AFTER_INNER, C_PASS_END,
+                C_NEWTON, C_COMMIT, C_DELTA, C_LIMITED };
+
+__device__ __forceinline__ void ctl_set(const CtlHandles& hd, HeatCtl* c, int body, bool on, bool count_entry) {
+    cudaGraphSetConditional(hd.h[body], on ? 1u : 0u);
+    if (on && count_entry) c->runs[body]++;
+}
+
+__global__ void heat_ctl_kernel(HeatCtl* c, double* scal, int phase, CtlHandles hd) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    switch (phase) {
+        case C_BEGIN: {  // after the set-up: Σ C T⁰, the gas cells and Δt in the scalars
+            c->heat0 = scal[S_HEAT0];
+            c->n_gas = scal[S_NGAS];
+            const bool skip = c->pin || c->n_gas == 0.0 || !(scal[S_DT] > 0.0);
+            c->skipped = skip;
+            c->passes = c->rounds = c->refinements = 0;
+            c->converged = skip ? 1 : 0;
+            c->ok = 1;
+            c->rel = c->delta = c->radiated = 0.0;
+            ctl_set(hd, c, B_MAIN, !skip, true);
+            ctl_set(hd, c, B_SKIP, skip, true);
+            break;
+        }
+        case C_NEWTON_BEGIN:  // after the first system (its two bounds in S_UB, S_TB)
+            c->pass_tol = fmax(c->tol, kFirstPassTol);
+            c->moved_prev = 0.0;
+            ctl_set(hd, c, B_PASS, c->max_passes > 0 && c->max_rounds > 0, false);
+            break;
+        case C_PASS_BEGIN:
+            c->runs[B_PASS]++;
+            c->passes++;
+            c->ref = 0;
+            c->prev = INFINITY;
+            ctl_set(hd, c, B_REFINE, true, false);
+            break;
+        case C_REFINE: {  // after the FP64 residual: stop, or scale the residual for an inner solve
+            c->runs[B_REFINE]++;
+            const double rr = scal[S_RR], bb = scal[S_BB], gam = scal[S_GAM], hm = scal[S_HM];
+            bool go = false;
+            if (!isfinite(rr) || !isfinite(bb) || !isfinite(gam) || !isfinite(hm)) {
+                c->ok = 0;
+            } else {
+                c->rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+                const double tol = c->pass_tol, ub = scal[S_UB], tb = scal[S_TB];
+                double worst = c->rel / tol;
+                if (ub > 0.0) worst = fmax(worst, sqrt(gam / ub) / tol);
+                if (tb > 0.0) worst = fmax(worst, sqrt(hm / tb) / tol);
+                if (!(worst <= 1.0 || rr == 0.0) && !(worst > 0.5 * c->prev) && c->rounds < c->max_rounds) {
+                    c->prev = worst;
+                    const double scale = sqrt(rr / fmax(1.0, c->n_gas));
+                    scal[S_SCALE] = scale;
+                    scal[S_ISCALE] = 1.0 / scale;
+                    c->eta = fmin(0.5, fmax(c->inner_floor, 0.5 / worst));
+                    c->max_it = c->max_rounds - c->rounds;
+                    go = true;
+                }
+            }
+            ctl_set(hd, c, B_INNER, go, true);
+            if (!go) ctl_set(hd, c, B_REFINE, false, false);
+            break;
+        }
+        case C_INNER_BEGIN: {  // after the scaled residual and its first preconditioner application
+            scal[S_RZC] = scal[S_RZN];
+            scal[S_BETA] = 0.0;
+            scal[S_PAR] = 0.0;
+            c->rr0 = scal[S_R32];
+            c->it = 0;
+            c->reached = 0;
+            ctl_set(hd, c, B_ROUND, c->rr0 > 0.0 && c->max_it > 0, false);
+            break;
+        }
+        case C_ROUND: {  // after a round: rotate its state, test the residual
+            c->runs[B_ROUND]++;
+            c->it++;
+            scal[S_RZP] = scal[S_RZC];
+            scal[S_RZC] = scal[S_RZN];
+            scal[S_PAR] = scal[S_PAR] != 0.0 ? 0.0 : 1.0;
+            const double pq = scal[S_PQ], rr = scal[S_RRI];
+            bool more = true;
+            if (!(pq > 0.0) || !isfinite(pq) || !isfinite(rr)) {
+                c->ok = 0;  // a breakdown: the solve's correction is dropped
+                scal[S_SCALE] = 0.0;
+                more = false;
+            } else if (rr <= c->eta * c->eta * c->rr0) {
+                c->reached = 1;
+                more = false;
+            } else if (c->it >= c->max_it) {
+                more = false;
+            }
+            ctl_set(hd, c, B_ROUND, more, false);
+            break;
+        }
+        case C_AFTER_INNER: {  // after the correction x += scale e
+            bool more = c->ok != 0;
+            if (c->ok) {
+                c->rounds += c->it;
+                c->refinements++;
+                // an intermediate pass (its tolerance far above the FP32 solve's floor) trusts the solve that reached
+                // its reduction; the final pass is always verified by another FP64 residual
+                if (c->reached && c->pass_tol >= kTrustedPassTol) {
+                    c->rel *= c->eta;
+                    more = false;
+                }
+            }
+            if (++c->ref >= kMaxRefinements) more = false;
+            ctl_set(hd, c, B_REFINE, more, false);
+            break;
+        }
+        case C_PASS_END:  // the pass's solve is done: its Newton update, unless the solve broke down
+            ctl_set(hd, c, B_NSYS, c->ok != 0, true);
+            if (!c->ok) ctl_set(hd, c, B_PASS, false, false);
+            break;
+        case C_NEWTON: {  // after the update and the next system: stop, or the next pass's tolerance and coarsening
+            const double rel_moved = c->heat0 > 0.0 ? scal[S_MOVED] / c->heat0 : 0.0;
+            bool more;
+            if (rel_moved <= c->nheat && scal[S_VIOL] == 0.0 && c->pass_tol <= c->tol) {
+                c->converged = 1;
+                more = false;
+            } else {
+                // the next pass is solved to tol once it is expected to move less than nheat (the passes' observed
+                // contraction times this pass's move), since only a pass solved to tol can end them
+                const double ratio = c->moved_prev > 0.0 ? fmin(1.0, fmax(0.01, rel_moved / c->moved_prev)) : 0.1;
+                c->moved_prev = rel_moved;
+                c->pass_tol = fmax(c->tol, fmin(kFirstPassTol, rel_moved));
+                if (ratio * rel_moved <= c->nheat) c->pass_tol = c->tol;
+                more = c->passes < c->max_passes && c->rounds < c->max_rounds;
+            }
+            ctl_set(hd, c, B_COARSEN, more, true);
+            ctl_set(hd, c, B_PASS, more, false);
+            break;
+        }
+        case C_COMMIT:
+            ctl_set(hd, c, B_CONV, c->converged != 0, true);
+            ctl_set(hd, c, B_LIM, !c->converged, true);
+            break;
+        case C_DELTA: {  // after the commit's sums (heat.rs:521-531)
+            const double rad = scal[S_RAD], gain = scal[S_GAIN], held = scal[S_HELD];
+            c->delta = -(gain + rad) / held;
+            c->radiated = rad;
+            scal[S_DELTA] = c->delta;
+            break;
+        }
+        case C_LIMITED:
+            c->radiated = scal[S_RAD];
+            break;
+    }
 }
 
 int grid_for(size_t n) {
@@ -809,6 +1039,16 @@ struct HeatSolver {
     float* ez = nullptr;          // sample collection: the iterate after each round's V-cycle
     float* vz = nullptr;          // the learned preconditioner's second V-cycle
     void* flush = nullptr;        // timing hook: a buffer larger than L2
+    // the device-controlled step: its control block, the captured graphs (one per state buffer the step updates),
+    // the extra streams its nested bodies are captured on, and each body's kernel count
+    HeatCtl* ctl = nullptr;
+    HeatCtl* hctl = nullptr;      // pinned host copy
+    std::map<const float*, cudaGraphExec_t> step_graphs;
+    cudaStream_t cap[6] = {};
+    long long body_launches[B_COUNT + 1] = {};  // [B_COUNT]: the graph's own top-level kernels
+    bool report_pending = false;  // the last step ran as a graph: its report is in ctl
+    cudaStream_t stream = nullptr;  // the owning context's stream
+    sr_heat_report report{};
 
     Red red(int slot) { return Red{part, counter, scal + slot}; }
 
@@ -820,6 +1060,11 @@ struct HeatSolver {
 };
 
 namespace {
+
+void set_scalar(HeatSolver* H, int slot, double value, cudaStream_t s) {
+    set_scalar_kernel<<<1, 32, 0, s>>>(H->scal, slot, value);
+    sr_note_launch();
+}
 
 void setup_step(HeatSolver* H, const float* U, const float* kappa, cudaStream_t s) {
     const HeatConst& K = H->K;
@@ -874,17 +1119,19 @@ void round_launches(HeatSolver* H, uint32_t precond, int parity, cudaStream_t s)
         sr_note_launch();
         return;
     }
-    // rz_old holds this round's <r, z>, rz_new the previous round's (then the next round's, after the preconditioner);
-    // the direction is read from one buffer and written to the other (neighbours read the old one)
-    float* pin = parity ? H->p2 : H->p32;
-    float* pout = parity ? H->p32 : H->p2;
-    spmv_dir_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->scal, rz_old, rz_new, H->z32, pin, pout, H->q32,
+    // the fused round: the state (<r, z> slots, which direction buffer is current) lives in the device scalars, so
+    // one captured graph serves every round
+    (void)rz_old;
+    (void)rz_new;
+    spmv_dir_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->mg.L[0], H->scal, H->z32, H->p32, H->p2, H->q32,
                                                     H->red(S_PQ), H->scal + S_BETA);
     sr_note_launch();
-    pcg_update4_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, rz_old, pout, H->q32, H->e32, H->r32,
+    pcg_update4_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, H->p32, H->p2, H->q32, H->e32, H->r32,
                                                        H->red(S_RRI));
     sr_note_launch();
-    precondition(H, precond, rz_new, s);
+    precondition(H, precond, S_RZN, s);
+    pcg_rotate_kernel<<<1, 32, 0, s>>>(H->scal);
+    sr_note_launch();
 }
 
 // A round as one CUDA graph launch (captured once per preconditioner and parity; every pointer it reads is fixed).
@@ -893,7 +1140,7 @@ void run_round(HeatSolver* H, uint32_t precond, int parity, cudaStream_t s) {
         round_launches(H, precond, parity, s);
         return;
     }
-    RoundGraph& g = H->graphs[precond][parity];
+    RoundGraph& g = H->graphs[precond][precond == SR_PRECOND_LEARNED ? parity : 0];
     if (!g.exec) {
         const long long before = (long long)sr_launches();
         cudaGraph_t graph;
@@ -918,8 +1165,6 @@ struct SolveResult {
     bool fallback = false;  // the learned preconditioner stalled and MG-PCG finished
 };
 
-constexpr double kFirstPassTol = 0.1;  // the first Newton pass's relative residual (and the loosest any pass asks)
-constexpr double kTrustedPassTol = 1e-5;  // passes this loose end on their FP32 solve's own test
 constexpr int kStallRounds = 24;  // learned: rounds after which a solve that has not gained 100x falls back
 
 // PCG on A32 e = r32 from e = 0 to a residual reduction `eta` or `max_it` rounds. Returns the rounds, -1 on a
@@ -927,12 +1172,14 @@ constexpr int kStallRounds = 24;  // learned: rounds after which a solve that ha
 // (a breakdown, or less than a 100x reduction after kStallRounds): plain MG-PCG then takes over.
 int inner_pcg(HeatSolver* H, uint32_t precond, double eta, int max_it, cudaStream_t s, bool* reached = nullptr) {
     if (reached) *reached = false;
-    precondition(H, precond, S_RZ0, s);
     if (precond == SR_PRECOND_LEARNED) {  // flexible CG forms its direction at the end of a round
+        precondition(H, precond, S_RZ0, s);
         pcg_direction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->scal, -1, S_RZ0, H->z32, H->p32);
         sr_note_launch();
     } else {  // the first round's fused direction is p = z
-        SR_CUDA_TRY(cudaMemsetAsync(H->scal + S_BETA, 0, sizeof(double), s));
+        precondition(H, precond, S_RZN, s);
+        pcg_start_kernel<<<1, 32, 0, s>>>(H->scal);
+        sr_note_launch();
     }
     H->read(S_R32, 1, s);  // <r, r> of the scaled residual (written by scale_kernel)
     const double rr0 = H->hscal[S_R32];
@@ -972,7 +1219,7 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
     double prev = INFINITY;
     const double ub = H->hscal[S_UB], tb = H->hscal[S_TB];
     for (int ref = 0; ref < 16; ref++) {
-        heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, dt, H->gas, H->c64, H->rhs, H->kx, H->ky, H->C,
+        heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, H->scal, H->gas, H->c64, H->rhs, H->kx, H->ky, H->C,
                                                                H->t, H->x, H->r64, H->red(S_RR));
         sr_note_launch();
         H->read(S_RR, 4, s);
@@ -989,7 +1236,9 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         if (worst > 0.5 * prev || R.rounds >= max_rounds) return R;  // stagnating, or out of rounds
         prev = worst;
         const double scale = sqrt(rr / (double)std::max(1, H->n_gas));
-        scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->red(S_R32));
+        set_scalar(H, S_SCALE, scale, s);
+        set_scalar(H, S_ISCALE, 1.0 / scale, s);
+        scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, H->scal, H->r32, H->e32, H->red(S_R32));
         sr_note_launch();
         const double eta = std::min(0.5, std::max(H->inner_floor, 0.5 / worst));
         bool reached = false;
@@ -1007,7 +1256,7 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
         }
         R.rounds += it;
         R.refinements++;
-        correction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->gas, H->e32, scale, H->x);
+        correction_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->gas, H->e32, H->scal, H->x);
         sr_note_launch();
         // an intermediate Newton pass (its tolerance far above the FP32 solve's floor) trusts the FP32 solve that
         // reached its reduction: the next pass starts from a fresh residual anyway; the final pass is always verified
@@ -1021,11 +1270,177 @@ SolveResult solve_pass(HeatSolver* H, uint32_t precond, double tol, int max_roun
 
 // A pass's system and its measures' bounds (read to the host), then every coarse level and the coarsest inverse.
 void build_system(HeatSolver* H, double dt, cudaStream_t s) {
-    heat_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->u, H->t0, H->kvac, H->c64,
+    set_scalar(H, S_DT, dt, s);
+    heat_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->scal, H->gas, H->C, H->t, H->u, H->t0, H->kvac, H->c64,
                                                        H->rhs, H->mg.L[0].c, H->x, H->red(S_UB));
     sr_note_launch();
     H->mg.coarsen(s);
     H->read(S_UB, 2, s);
+}
+
+// Appends a conditional node of `type` steered by `h` after everything captured so far on `s` (which is capturing),
+// makes the stream's later work follow it, and returns its body graph.
+cudaGraph_t capture_conditional(cudaStream_t s, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type) {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    SR_CUDA_TRY(cudaStreamGetCaptureInfo(s, &st, nullptr, &g, &deps, &nd));
+    SR_REQUIRE(st == cudaStreamCaptureStatusActive, "a conditional node outside a stream capture");
+    cudaGraphNodeParams p{};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = type;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    SR_CUDA_TRY(cudaGraphAddNode(&node, g, deps, nd, &p));
+    SR_CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return p.conditional.phGraph_out[0];
+}
+
+// Captures `body(stream)` into the body graph `g` on stream `cs`; returns the kernels it launched.
+template <class F>
+long long capture_body(cudaGraph_t g, cudaStream_t cs, F body) {
+    const long long before = (long long)sr_launches();
+    SR_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    body(cs);
+    cudaGraph_t out;
+    SR_CUDA_TRY(cudaStreamEndCapture(cs, &out));
+    const long long n = (long long)sr_launches() - before;
+    sr_note_launches(-n);  // captured, not launched
+    return n;
+}
+
+void ctl_launch(HeatSolver* H, int phase, const CtlHandles& hd, cudaStream_t s) {
+    heat_ctl_kernel<<<1, 32, 0, s>>>(H->ctl, H->scal, phase, hd);
+    sr_note_launch();
+}
+
+// The whole implicit step (MG or Jacobi preconditioner) appended to the capture in progress on `s`, whose root graph
+// is `root` (the conditional handles belong to it): set-up, Δt from the device record, the device-controlled Newton
+// passes, refinements and PCG rounds, and the commit. The state buffer `U` and the opacity plane are fixed in it.
+void capture_heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev, cudaStream_t s,
+                       cudaGraph_t root) {
+    CtlHandles hd;
+    for (int b = 0; b < B_COUNT; b++) SR_CUDA_TRY(cudaGraphConditionalHandleCreate(&hd.h[b], root, 0, 0));
+    const uint32_t precond = H->precond;
+    const size_t nf = (size_t)(H->w + 1) * H->h + (size_t)H->w * (H->h + 1);
+    long long* nb = H->body_launches;
+    const long long top0 = (long long)sr_launches();
+    setup_step(H, U, kappa, s);
+    SR_CUDA_TRY(cudaMemcpyAsync(H->scal + S_DT, dt_dev, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ctl_launch(H, C_BEGIN, hd, s);
+    const long long top1 = (long long)sr_launches();
+    nb[B_MAIN] = capture_body(capture_conditional(s, hd.h[B_MAIN], cudaGraphCondTypeIf), H->cap[0], [&](cudaStream_t s0) {
+        if (precond != SR_PRECOND_JACOBI) {
+            warm_start_kernel<<<H->grid, RED_THREADS, 0, s0>>>(H->K, H->scal, H->gas, H->t0, H->rate, H->t, H->u);
+            sr_note_launch();
+        }
+        heat_system_kernel<<<H->grid, RED_THREADS, 0, s0>>>(H->K, H->scal, H->gas, H->C, H->t, H->u, H->t0, H->kvac,
+                                                            H->c64, H->rhs, H->mg.L[0].c, H->x, H->red(S_UB));
+        sr_note_launch();
+        H->mg.coarsen(s0);
+        ctl_launch(H, C_NEWTON_BEGIN, hd, s0);
+        nb[B_PASS] = capture_body(capture_conditional(s0, hd.h[B_PASS], cudaGraphCondTypeWhile), H->cap[1],
+                                  [&](cudaStream_t s1) {
+            ctl_launch(H, C_PASS_BEGIN, hd, s1);
+            nb[B_REFINE] = capture_body(capture_conditional(s1, hd.h[B_REFINE], cudaGraphCondTypeWhile), H->cap[2],
+                                        [&](cudaStream_t s2) {
+                heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s2>>>(H->K, H->scal, H->gas, H->c64, H->rhs, H->kx,
+                                                                         H->ky, H->C, H->t, H->x, H->r64, H->red(S_RR));
+                sr_note_launch();
+                ctl_launch(H, C_REFINE, hd, s2);
+                nb[B_INNER] = capture_body(capture_conditional(s2, hd.h[B_INNER], cudaGraphCondTypeIf), H->cap[3],
+                                           [&](cudaStream_t s3) {
+                    scale_kernel<<<H->grid, RED_THREADS, 0, s3>>>(H->n, H->r64, H->scal, H->r32, H->e32, H->red(S_R32));
+                    sr_note_launch();
+                    precondition(H, precond, S_RZN, s3);
+                    ctl_launch(H, C_INNER_BEGIN, hd, s3);
+                    nb[B_ROUND] = capture_body(capture_conditional(s3, hd.h[B_ROUND], cudaGraphCondTypeWhile), H->cap[4],
+                                               [&](cudaStream_t s4) {
+                        spmv_dir_kernel<<<H->grid, RED_THREADS, 0, s4>>>(H->mg.L[0], H->scal, H->z32, H->p32, H->p2,
+                                                                          H->q32, H->red(S_PQ), H->scal + S_BETA);
+                        sr_note_launch();
+                        pcg_update4_kernel<<<H->grid, RED_THREADS, 0, s4>>>(H->n, H->scal, H->p32, H->p2, H->q32,
+                                                                             H->e32, H->r32, H->red(S_RRI));
+                        sr_note_launch();
+                        precondition(H, precond, S_RZN, s4);
+                        ctl_launch(H, C_ROUND, hd, s4);
+                    });
+                    correction_kernel<<<H->grid, RED_THREADS, 0, s3>>>(H->n, H->gas, H->e32, H->scal, H->x);
+                    sr_note_launch();
+                    ctl_launch(H, C_AFTER_INNER, hd, s3);
+                });
+            });
+            ctl_launch(H, C_PASS_END, hd, s1);
+            nb[B_NSYS] = capture_body(capture_conditional(s1, hd.h[B_NSYS], cudaGraphCondTypeIf), H->cap[2],
+                                      [&](cudaStream_t s2) {
+                newton_system_kernel<<<H->grid, RED_THREADS, 0, s2>>>(H->K, H->cfg.newton_cell, H->scal, H->gas, H->C,
+                                                                       H->t0, H->kvac, H->t, H->u, H->x, H->c64,
+                                                                       H->rhs, H->mg.L[0].c, H->red(S_MOVED));
+                sr_note_launch();
+                ctl_launch(H, C_NEWTON, hd, s2);
+                nb[B_COARSEN] = capture_body(capture_conditional(s2, hd.h[B_COARSEN], cudaGraphCondTypeIf), H->cap[3],
+                                             [&](cudaStream_t s3) { H->mg.coarsen(s3); });
+            });
+        });
+        ctl_launch(H, C_COMMIT, hd, s0);
+        nb[B_CONV] = capture_body(capture_conditional(s0, hd.h[B_CONV], cudaGraphCondTypeIf), H->cap[1],
+                                  [&](cudaStream_t s1) {
+            heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s1>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx,
+                                                                   H->fy);
+            sr_note_launch();
+            commit_sums_kernel<<<H->grid, RED_THREADS, 0, s1>>>(H->K, H->scal, H->gas, H->C, H->t, H->t0, H->u,
+                                                                H->kvac, H->red(S_RAD));
+            sr_note_launch();
+            ctl_launch(H, C_DELTA, hd, s1);
+            commit_apply_kernel<<<H->grid, RED_THREADS, 0, s1>>>(H->K, H->scal, H->gas, H->C, H->t, H->t0, U, H->rate);
+            sr_note_launch();
+        });
+        nb[B_LIM] = capture_body(capture_conditional(s0, hd.h[B_LIM], cudaGraphCondTypeIf), H->cap[1],
+                                 [&](cudaStream_t s1) {
+            limited_scale_kernel<<<H->grid, RED_THREADS, 0, s1>>>(H->K, H->scal, H->gas, H->kx, H->ky, H->u, H->C,
+                                                                  H->t0, H->lscale);
+            sr_note_launch();
+            heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s1>>>(H->K, H->gas, H->kx, H->ky, H->u, H->lscale, H->fx,
+                                                                   H->fy);
+            sr_note_launch();
+            limited_apply_kernel<<<H->grid, RED_THREADS, 0, s1>>>(H->K, H->scal, H->gas, H->kx, H->ky, H->u,
+                                                                  H->lscale, U, H->red(S_RAD));
+            sr_note_launch();
+            zero_kernel<<<H->grid, RED_THREADS, 0, s1>>>(H->rate, H->n);
+            sr_note_launch();
+            ctl_launch(H, C_LIMITED, hd, s1);
+        });
+    });
+    nb[B_SKIP] = capture_body(capture_conditional(s, hd.h[B_SKIP], cudaGraphCondTypeIf), H->cap[0],
+                              [&](cudaStream_t s0) {
+        heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s0>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx, H->fy);
+        sr_note_launch();
+    });
+    nb[B_COUNT] = top1 - top0;
+    sr_note_launches(-(top1 - top0));  // captured, not launched
+}
+
+// The control block's configuration for the next steps.
+void ctl_configure(HeatSolver* H, cudaStream_t s) {
+    HeatCtl c{};
+    c.tol = H->cfg.solve_tol;
+    c.nheat = H->cfg.newton_heat;
+    c.ncell = H->cfg.newton_cell;
+    c.inner_floor = H->inner_floor;
+    c.max_passes = (int)H->max_passes;
+    c.max_rounds = (int)H->max_rounds;
+    c.pin = H->cfg.pin_temperature ? 1 : 0;
+    *H->hctl = c;
+    SR_CUDA_TRY(cudaMemcpyAsync(H->ctl, H->hctl, sizeof(HeatCtl), cudaMemcpyHostToDevice, s));
+    SR_CUDA_TRY(cudaStreamSynchronize(s));
+}
+
+void drop_step_graphs(HeatSolver* H) {
+    if (!H->step_graphs.empty() && H->stream) cudaStreamSynchronize(H->stream);  // none of them still running
+    for (auto& kv : H->step_graphs) cudaGraphExecDestroy(kv.second);
+    H->step_graphs.clear();
 }
 
 }  // namespace
@@ -1038,6 +1453,7 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         H->h = (int)cfg.height;
         H->n = (size_t)H->w * H->h;
         SR_REQUIRE(cfg.precond != SR_PRECOND_LEARNED, "the learned preconditioner is loaded after creation");
+        H->stream = s;
         H->precond = cfg.precond;
         H->max_passes = cfg.max_passes ? cfg.max_passes : 128;
         H->max_rounds = cfg.max_rounds ? cfg.max_rounds : 4096;
@@ -1076,6 +1492,10 @@ HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s) {
         SR_CUDA_TRY(cudaMalloc(&H->scal, sizeof(double) * S_COUNT));
         SR_CUDA_TRY(cudaMemset(H->scal, 0, sizeof(double) * S_COUNT));
         SR_CUDA_TRY(cudaMallocHost(&H->hscal, sizeof(double) * S_COUNT));
+        SR_CUDA_TRY(cudaMalloc(&H->ctl, sizeof(HeatCtl)));
+        SR_CUDA_TRY(cudaMemset(H->ctl, 0, sizeof(HeatCtl)));
+        SR_CUDA_TRY(cudaMallocHost(&H->hctl, sizeof(HeatCtl)));
+        for (cudaStream_t& c : H->cap) SR_CUDA_TRY(cudaStreamCreateWithFlags(&c, cudaStreamNonBlocking));
         H->mg.create(H->w, H->h, (int)cfg.mg_pre, (int)cfg.mg_post);
         H->mg.omega = cfg.mg_omega > 0.0 ? (float)cfg.mg_omega : 1.0f;
         H->inner_floor = cfg.inner_tol > 0.0 ? cfg.inner_tol : 1e-5;
@@ -1093,6 +1513,11 @@ void heat_destroy(HeatSolver* H) {
     for (auto& row : H->graphs)
         for (auto& g : row)
             if (g.exec) cudaGraphExecDestroy(g.exec);
+    drop_step_graphs(H);
+    cudaFree(H->ctl);
+    if (H->hctl) cudaFreeHost(H->hctl);
+    for (cudaStream_t c : H->cap)
+        if (c) cudaStreamDestroy(c);
     cudaFree(H->gas);
     double* d64[] = {H->t0, H->C, H->t, H->u, H->ksum, H->kvac, H->c64, H->rhs, H->x, H->r64, H->lscale, H->rate,
                      H->kx, H->ky};
@@ -1115,6 +1540,7 @@ void heat_destroy(HeatSolver* H) {
 void heat_set_precond(HeatSolver* H, uint32_t precond) {
     if (precond == SR_PRECOND_LEARNED && !H->lapply)
         throw SrError{SR_E_UNSUPPORTED, "the learned preconditioner is not attached (sr_attach_learner)"};
+    if (precond != H->precond) drop_step_graphs(H);  // a captured step holds its preconditioner
     H->precond = precond;
 }
 
@@ -1142,14 +1568,16 @@ int heat_collect(HeatSolver* H, Learner* L, const float* U, const float* kappa, 
     H->read(S_HEAT0, 2, s);
     H->n_gas = (int)H->hscal[S_NGAS];
     build_system(H, dt, s);
-    heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->c64, H->rhs, H->kx, H->ky, H->C, H->t,
-                                                           H->x, H->r64, H->red(S_RR));
+    heat_residual64_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->scal, H->gas, H->c64, H->rhs, H->kx, H->ky, H->C,
+                                                           H->t, H->x, H->r64, H->red(S_RR));
     sr_note_launch();
     H->read(S_RR, 1, s);
     const double rr = H->hscal[S_RR];
     if (!(rr > 0.0) || !isfinite(rr)) return 0;
     const double scale = sqrt(rr / (double)std::max(1, H->n_gas));
-    scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, 1.0 / scale, H->r32, H->e32, H->red(S_R32));
+    set_scalar(H, S_SCALE, scale, s);
+    set_scalar(H, S_ISCALE, 1.0 / scale, s);
+    scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->n, H->r64, H->scal, H->r32, H->e32, H->red(S_R32));
     sr_note_launch();
     if (!H->ez) SR_CUDA_TRY(cudaMalloc(&H->ez, sizeof(float) * H->n));
     // after each V-cycle z_k = M_mg r_k: the sample (r_k − A z_k, e_k + z_k); q32 is free until the next round's SpMV
@@ -1190,6 +1618,7 @@ void heat_reset(HeatSolver* H, cudaStream_t s) { SR_CUDA_TRY(cudaMemsetAsync(H->
 void heat_set_limits(HeatSolver* H, uint32_t max_passes, uint32_t max_rounds) {
     H->max_passes = max_passes;
     H->max_rounds = max_rounds;
+    drop_step_graphs(H);  // the next step captures again, with the new limits in its control block
 }
 
 void heat_read_flux(HeatSolver* H, float* fx, float* fy) {
@@ -1198,8 +1627,65 @@ void heat_read_flux(HeatSolver* H, float* fx, float* fy) {
     if (fy) SR_CUDA_TRY(cudaMemcpy(fy, H->fy, sizeof(float) * ny, cudaMemcpyDeviceToHost));
 }
 
+// Reads the device-controlled steps' control block: the last step's report, and the kernels its bodies launched since
+// the last read (added to the library's launch count).
+void heat_sync_report(HeatSolver* H, cudaStream_t s) {
+    if (!H->report_pending) return;
+    SR_CUDA_TRY(cudaMemcpyAsync(H->hctl, H->ctl, sizeof(HeatCtl), cudaMemcpyDeviceToHost, s));
+    SR_CUDA_TRY(cudaMemsetAsync(H->ctl->runs, 0, sizeof(H->ctl->runs), s));
+    SR_CUDA_TRY(cudaStreamSynchronize(s));
+    const HeatCtl& c = *H->hctl;
+    long long n = 0;
+    for (int b = 0; b < B_COUNT; b++) n += (long long)c.runs[b] * H->body_launches[b];
+    sr_note_launches(n);
+    sr_heat_report R{};
+    R.precond = H->precond;
+    R.dt = c.skipped ? 0.0 : H->hscal[S_DT];
+    R.passes = (uint32_t)c.passes;
+    R.rounds = (uint32_t)c.rounds;
+    R.refinements = (uint32_t)c.refinements;
+    R.converged = (uint32_t)c.converged;
+    R.delta = c.delta;
+    R.radiated = c.radiated;
+    R.rel_residual = c.rel;
+    H->report = R;
+    H->report_pending = false;
+}
+
 void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev, cudaStream_t s,
                sr_heat_report* rep) {
+    if (H->precond != SR_PRECOND_LEARNED && H->use_graphs && H->mg.tuned) {
+        // the device-controlled step: captured once per state buffer, then replayed with no host round trip
+        auto it = H->step_graphs.find(U);
+        if (it == H->step_graphs.end()) {
+            heat_sync_report(H, s);
+            ctl_configure(H, s);
+            cudaGraph_t g;
+            SR_CUDA_TRY(cudaGraphCreate(&g, 0));
+            SR_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            try {
+                capture_heat_step(H, U, kappa, dt_dev, s, g);
+            } catch (...) {
+                cudaGraph_t dead;
+                cudaStreamEndCapture(s, &dead);
+                cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t out;
+            SR_CUDA_TRY(cudaStreamEndCapture(s, &out));
+            cudaGraphExec_t exec;
+            const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            SR_CUDA_TRY(e);
+            it = H->step_graphs.emplace(U, exec).first;
+        }
+        SR_CUDA_TRY(cudaGraphLaunch(it->second, s));
+        sr_note_launches(H->body_launches[B_COUNT]);
+        H->report_pending = true;
+        (void)rep;
+        return;
+    }
+    heat_sync_report(H, s);
     sr_heat_report R{};
     R.precond = H->precond;
     setup_step(H, U, kappa, s);
@@ -1213,13 +1699,14 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx,
                                                                H->fy);
         sr_note_launch();
+        R.converged = 1;
+        H->report = R;
         *rep = R;
-        rep->converged = 1;
         return;
     }
     R.dt = dt;
     if (H->precond != SR_PRECOND_JACOBI) {
-        warm_start_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->t0, H->rate, H->t, H->u);
+        warm_start_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->scal, H->gas, H->t0, H->rate, H->t, H->u);
         sr_note_launch();
     }
     uint32_t passes = 0, rounds = 0;
@@ -1241,7 +1728,7 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         R.rel_residual = S.rel;
         if (S.fallback) R.fallback_used = 1;
         if (!S.ok) break;
-        newton_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, ncell, dt, H->gas, H->C, H->t0,
+        newton_system_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, ncell, H->scal, H->gas, H->C, H->t0,
                                                               H->kvac, H->t, H->u, H->x, H->c64, H->rhs,
                                                               H->mg.L[0].c, H->red(S_MOVED));
         sr_note_launch();
@@ -1264,25 +1751,26 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
     if (converged) {
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, nullptr, H->fx, H->fy);
         sr_note_launch();
-        commit_sums_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->C, H->t, H->t0, H->u, H->kvac,
+        commit_sums_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->scal, H->gas, H->C, H->t, H->t0, H->u, H->kvac,
                                                            H->red(S_RAD));
         sr_note_launch();
         H->read(S_RAD, 3, s);
         const double rad = H->hscal[S_RAD], gain = H->hscal[S_GAIN], held = H->hscal[S_HELD];
         const double delta = -(gain + rad) / held;
-        commit_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, delta, dt, H->gas, H->C, H->t, H->t0, U, H->rate);
+        set_scalar(H, S_DELTA, delta, s);
+        commit_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->scal, H->gas, H->C, H->t, H->t0, U, H->rate);
         sr_note_launch();
         R.converged = 1;
         R.delta = delta;
         R.radiated = rad;
     } else {
-        limited_scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->C, H->t0,
+        limited_scale_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->scal, H->gas, H->kx, H->ky, H->u, H->C, H->t0,
                                                              H->lscale);
         sr_note_launch();
         heat_flux_kernel<<<grid_for(nf), RED_THREADS, 0, s>>>(H->K, H->gas, H->kx, H->ky, H->u, H->lscale, H->fx,
                                                                H->fy);
         sr_note_launch();
-        limited_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, dt, H->gas, H->kx, H->ky, H->u, H->lscale, U,
+        limited_apply_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->K, H->scal, H->gas, H->kx, H->ky, H->u, H->lscale, U,
                                                              H->red(S_RAD));
         sr_note_launch();
         SR_CUDA_TRY(cudaMemsetAsync(H->rate, 0, sizeof(double) * H->n, s));
@@ -1292,8 +1780,16 @@ void heat_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev
         R.radiated = H->hscal[S_RAD];
     }
     SR_CUDA_TRY(cudaGetLastError());
+    H->report = R;
     *rep = R;
 }
+
+void heat_report(HeatSolver* H, cudaStream_t s, sr_heat_report* rep) {
+    heat_sync_report(H, s);
+    *rep = H->report;
+}
+
+void heat_account_launches(HeatSolver* H, cudaStream_t s) { heat_sync_report(H, s); }
 
 void heat_first_solve(HeatSolver* H, const float* U, const float* kappa, double dt, uint32_t precond, cudaStream_t s,
                       double* ms, uint32_t* rounds, double* rel_residual, double* x, uint32_t* fallback) {

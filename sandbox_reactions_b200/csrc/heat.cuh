@@ -11,6 +11,10 @@ void heat_destroy(HeatSolver* hs);
 // One implicit step of length *dt_dev on the 4 planes U (E changes), κ from `kappa` (W*H) or cfg.kappa0.
 void heat_step(HeatSolver* hs, float* U, const float* kappa, const double* dt_dev, cudaStream_t s, sr_heat_report* rep);
 void heat_read_flux(HeatSolver* hs, float* fx, float* fy);
+// The last implicit step's report (waits for it when the step ran as a captured graph).
+void heat_report(HeatSolver* hs, cudaStream_t s, sr_heat_report* rep);
+// Adds the kernels the captured steps launched since the last count to the library's launch count (waits for them).
+void heat_account_launches(HeatSolver* hs, cudaStream_t s);
 // Forgets the last step's rates (a new state was uploaded).
 void heat_reset(HeatSolver* hs, cudaStream_t s);
 void heat_set_precond(HeatSolver* hs, uint32_t precond);
