@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -55,6 +56,9 @@ struct sr_ctx {
     sr_learner* learner = nullptr;  // attached learned preconditioner (not owned)
     sr_heat_report heat_report{};
     bool uploaded = false;
+    cudaGraphExec_t step_graph[2] = {nullptr, nullptr};  // a whole step from state buffer 0 / 1, captured on first use
+    long long step_launches = 0;
+    unsigned generation = 0;  // counts the invalidations of captured steps (a batch's graph checks it)
     // timing
     bool timing = false;
     std::vector<cudaEvent_t> events;
@@ -104,6 +108,16 @@ static void dalloc(T** p, size_t count) {
     SR_CUDA_TRY(cudaMemset(*p, 0, sizeof(T) * (count ? count : 1)));
 }
 
+static void drop_step_graphs(sr_ctx* c) {
+    c->generation++;
+    for (auto& g : c->step_graph)
+        if (g) {
+            cudaStreamSynchronize(c->stream);
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
 static void ctx_free(sr_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
@@ -115,6 +129,7 @@ static void ctx_free(sr_ctx* c) {
     if (c->grav_ready) c->grav.destroy();
     cudaFree(c->part_d); cudaFree(c->part_best); cudaFree(c->part_idx); cudaFree(c->hreport); cudaFree(c->herr);
     cudaFree(c->rec); cudaFree(c->part_rate); cudaFree(c->part_g); cudaFree(c->part_nf);
+    drop_step_graphs(c);
     if (c->heat) heat_destroy(c->heat);
     for (auto e : c->events) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -175,12 +190,12 @@ static cudaEvent_t event_at(sr_ctx* c, size_t i) {
     return c->events[i];
 }
 
-static HydroArgs hydro_args(sr_ctx* c) {
+static HydroArgs hydro_args(sr_ctx* c, int cur) {
     HydroArgs A{};
     A.H = c->H;
     A.dt = &c->rec->dt;
-    A.U = c->U[c->cur];
-    A.Uout = c->U[1 - c->cur];
+    A.U = c->U[cur];
+    A.Uout = c->U[1 - cur];
     A.gx = c->cfg.gravity ? c->gx : nullptr;
     A.gy = c->cfg.gravity ? c->gy : nullptr;
     A.src = c->src;
@@ -195,9 +210,115 @@ static HydroArgs hydro_args(sr_ctx* c) {
     return A;
 }
 
-static void run_steps(sr_ctx* c, uint32_t steps) {
+// One step's launches on `s` from state buffer `cur`, in the reference's pass order P1 → P2 → P4 → P5 → P8 → P9
+// (reference/mod.rs:264-297). With `root` the launches are captured into that graph and P5 is the device-controlled
+// step (heat_capture_step); otherwise they run now, P5 by heat_step. `mark(slot)` is called at the pass boundaries
+// (0 start, 1 after P2, 2 hydro update start, 3 its end, 4 after P4, 5 after P5, 6 after P8/P9).
+template <class Mark>
+static long long enqueue_step(sr_ctx* c, int cur, cudaStream_t s, cudaGraph_t root, Mark mark) {
+    long long heat_top = 0;  // kernels of a captured implicit step outside its loops
     const sr_config& k = c->cfg;
+    float* U = c->U[cur];
+    mark(0);
+    dt_advance_launch(c->rec, s);
+    if (k.gravity) c->grav.solve(U, c->phi, c->gx, c->gy, s);
+    mark(1);
+    if (k.hydro) {
+        HydroArgs A = hydro_args(c, cur);
+        if (k.gravity) {
+            hydro_launch(kHydroSource, A, s);
+            c->grav.solve(c->src, c->phim, c->gxm, c->gym, s);
+            mark(2);
+            hydro_launch(kHydroUpdateGrav, A, s);
+            mark(3);
+            hydro_finalize_launch(A, 1, s);
+        } else {
+            mark(2);
+            hydro_launch(kHydroUpdate, A, s);
+            mark(3);
+            hydro_finalize_launch(A, 0, s);
+        }
+        U = c->U[1 - cur];
+    } else {
+        mark(2);
+        mark(3);
+    }
+    mark(4);
+    if (k.heat) {
+        const float* kappa = k.opacity_plane ? c->kappa : nullptr;
+        if (root) heat_top = heat_capture_step(c->heat, U, kappa, &c->rec->dt, s, root);
+        else heat_step(c->heat, U, kappa, &c->rec->dt, s, &c->heat_report);
+    }
+    mark(5);
+    floors_dt_launch(c->H, U, k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 1, c->part_rate, c->part_g,
+                     c->part_nf, k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec, s);
+    mark(6);
+    return heat_top;
+}
+
+// Whether a whole step can run as one captured graph: P5 (when on) must run under device control.
+static bool capturable(sr_ctx* c) { return !c->cfg.heat || heat_capturable(c->heat); }
+
+// Appends one whole step from state buffer `cur` to the capture in progress on `s` (root graph `root`); returns the
+// kernels one replay launches outside the implicit step's loops.
+long long sr_ctx_capture_step(sr_ctx* c, int cur, cudaStream_t s, cudaGraph_t root) {
+    const long long before = (long long)sr_launches();
+    const long long heat_top = enqueue_step(c, cur, s, root, [](int) {});
+    const long long n = (long long)sr_launches() - before;
+    sr_note_launches(-n);  // captured, not launched
+    return n + heat_top;
+}
+
+// Readies `c` for captures of its whole step (the implicit step's control block); false when it cannot be captured.
+bool sr_ctx_prepare_capture(sr_ctx* c) {
+    if (!capturable(c)) return false;
+    if (c->cfg.heat) heat_prepare_capture(c->heat, c->stream);
+    return true;
+}
+
+// After `steps` whole steps ran as graphs: the state buffer, the implicit step's pending report, the launch count.
+void sr_ctx_graph_steps_done(sr_ctx* c, uint32_t steps, long long launches_per_step) {
+    if (c->cfg.hydro && (steps & 1)) c->cur = 1 - c->cur;
+    if (c->cfg.heat && steps) heat_graph_launched(c->heat);
+    sr_note_launches(launches_per_step * (long long)steps);
+}
+
+static void run_steps(sr_ctx* c, uint32_t steps) {
     const unsigned long long launches0 = sr_launches();
+    // without timing, after the first step (which tunes the multigrid), every step is one captured graph
+    if (!c->timing && steps && capturable(c)) {
+        if (!c->step_graph[c->cur]) {
+            sr_ctx_prepare_capture(c);
+            cudaGraph_t g;
+            SR_CUDA_TRY(cudaGraphCreate(&g, 0));
+            SR_CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            long long n = 0;
+            try {
+                n = sr_ctx_capture_step(c, c->cur, c->stream, g);
+            } catch (...) {
+                cudaGraph_t dead;
+                cudaStreamEndCapture(c->stream, &dead);
+                cudaGraphDestroy(g);
+                throw;
+            }
+            cudaGraph_t out;
+            SR_CUDA_TRY(cudaStreamEndCapture(c->stream, &out));
+            const cudaError_t e = cudaGraphInstantiate(&c->step_graph[c->cur], g, 0);
+            cudaGraphDestroy(g);
+            SR_CUDA_TRY(e);
+            c->step_launches = n;
+        }
+        for (uint32_t s = 0; s < steps; s++) {
+            if (!c->step_graph[c->cur]) break;
+            SR_CUDA_TRY(cudaGraphLaunch(c->step_graph[c->cur], c->stream));
+            sr_ctx_graph_steps_done(c, 1, c->step_launches);
+            if (!c->step_graph[c->cur] && s + 1 < steps) {  // the other state buffer's graph, captured on first use
+                run_steps(c, steps - s - 1);
+                return;
+            }
+        }
+        return;
+    }
     // event slots per step: 0 start, 1 after P2, 2 hydro update start, 3 hydro update end, 4 after P4, 5 after P5,
     // 6 after P8/P9
     const int E = 7;
@@ -205,37 +326,8 @@ static void run_steps(sr_ctx* c, uint32_t steps) {
         auto mark = [&](int slot) {
             if (c->timing) SR_CUDA_TRY(cudaEventRecord(event_at(c, (size_t)s * E + slot), c->stream));
         };
-        mark(0);
-        dt_advance_launch(c->rec, c->stream);
-        if (k.gravity) c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
-        mark(1);
-        if (k.hydro) {
-            HydroArgs A = hydro_args(c);
-            if (k.gravity) {
-                hydro_launch(kHydroSource, A, c->stream);
-                c->grav.solve(c->src, c->phim, c->gxm, c->gym, c->stream);
-                mark(2);
-                hydro_launch(kHydroUpdateGrav, A, c->stream);
-                mark(3);
-                hydro_finalize_launch(A, 1, c->stream);
-            } else {
-                mark(2);
-                hydro_launch(kHydroUpdate, A, c->stream);
-                mark(3);
-                hydro_finalize_launch(A, 0, c->stream);
-            }
-            c->cur = 1 - c->cur;
-        } else {
-            mark(2);
-            mark(3);
-        }
-        mark(4);
-        if (k.heat) heat_step(c->heat, planes(c), k.opacity_plane ? c->kappa : nullptr, &c->rec->dt, c->stream,
-                              &c->heat_report);
-        mark(5);
-        floors_dt_launch(c->H, planes(c), k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 1, c->part_rate,
-                         c->part_g, c->part_nf, k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec, c->stream);
-        mark(6);
+        enqueue_step(c, c->cur, c->stream, nullptr, mark);
+        if (c->cfg.hydro) c->cur = 1 - c->cur;
         SR_CUDA_TRY(cudaGetLastError());
     }
     if (c->timing && steps) {
@@ -259,7 +351,7 @@ static void run_steps(sr_ctx* c, uint32_t steps) {
             SR_CUDA_TRY(cudaEventElapsedTime(&total, c->events[(size_t)s * E], c->events[(size_t)s * E + 6]));
             t.total_ms += total;
         }
-        t.hydro_update_launches = k.hydro ? steps : 0;
+        t.hydro_update_launches = c->cfg.hydro ? steps : 0;
         t.kernel_launches = sr_launches() - launches0;
     }
 }
@@ -392,11 +484,9 @@ sr_status sr_upload_opacity(sr_ctx* c, const float* kappa) {
     });
 }
 
-sr_status sr_step(sr_ctx* c, uint32_t steps) {
+// The checks after steps ran (the stream idle): a bounded wait that gave up, then the non-finite guard.
+static sr_status after_steps(sr_ctx* c) {
     sr_status st = guarded(c, [&] {
-        SR_REQUIRE(c->uploaded, "sr_step: no state uploaded");
-        run_steps(c, steps);
-        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
         int herr = 0;
         SR_CUDA_TRY(cudaMemcpy(&herr, c->herr, sizeof herr, cudaMemcpyDeviceToHost));
         if (herr) {
@@ -416,6 +506,16 @@ sr_status sr_step(sr_ctx* c, uint32_t steps) {
         return SR_E_NONFINITE;
     }
     return SR_OK;
+}
+
+sr_status sr_step(sr_ctx* c, uint32_t steps) {
+    sr_status st = guarded(c, [&] {
+        SR_REQUIRE(c->uploaded, "sr_step: no state uploaded");
+        run_steps(c, steps);
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+    if (st != SR_OK) return st;
+    return after_steps(c);
 }
 
 sr_status sr_read_dt(sr_ctx* c, sr_dt_report* out) {
@@ -464,6 +564,7 @@ sr_status sr_heat_flux(sr_ctx* c, float* fx, float* fy) {
 sr_status sr_set_edge_mode(sr_ctx* c, uint32_t edge) {
     return guarded(c, [&] {
         SR_REQUIRE(edge <= SR_EDGE_LEAVE, "unknown edge mode");
+        drop_step_graphs(c);  // the captured steps hold the edge mode
         c->cfg.edge = edge;
         c->H.edge = (int)edge;
     });
@@ -473,6 +574,7 @@ sr_status sr_set_heat_precond(sr_ctx* c, uint32_t precond) {
     return guarded(c, [&] {
         SR_REQUIRE(precond <= SR_PRECOND_LEARNED, "unknown preconditioner");
         SR_REQUIRE(c->cfg.heat, "sr_set_heat_precond: the context runs no heat pass");
+        drop_step_graphs(c);
         c->cfg.precond = precond;
         heat_set_precond(c->heat, precond);
     });
@@ -482,6 +584,7 @@ sr_status sr_set_heat_limits(sr_ctx* c, uint32_t max_passes, uint32_t max_rounds
     return guarded(c, [&] {
         SR_REQUIRE(max_passes >= 1 && max_rounds >= 1, "heat limits must be >= 1");
         SR_REQUIRE(c->cfg.heat, "sr_set_heat_limits: the context runs no heat pass");
+        drop_step_graphs(c);
         c->cfg.max_passes = max_passes;
         c->cfg.max_rounds = max_rounds;
         heat_set_limits(c->heat, max_passes, max_rounds);
@@ -603,6 +706,7 @@ sr_status sr_learner_loss_grad(sr_learner* l, const float* feats, const float* t
 sr_status sr_attach_learner(sr_ctx* c, sr_learner* l) {
     return guarded(c, [&] {
         SR_REQUIRE(c->cfg.heat, "sr_attach_learner: the context runs no heat pass");
+        drop_step_graphs(c);
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
         heat_attach_learned(c->heat, l ? l->L : nullptr);
         c->learner = l;
@@ -611,6 +715,17 @@ sr_status sr_attach_learner(sr_ctx* c, sr_learner* l) {
 }
 
 const char* sr_last_error(const sr_ctx* c) { return c ? c->error.c_str() : g_create_error.c_str(); }
+
+}  // extern "C"
+
+// ---- for the batch (batch.cu): one captured graph over many contexts' whole steps
+sr_status sr_ctx_after_steps(sr_ctx* c) { return after_steps(c); }
+unsigned sr_ctx_generation(const sr_ctx* c) { return c->generation; }
+int sr_ctx_state(const sr_ctx* c) { return c->cur; }
+bool sr_ctx_uploaded(const sr_ctx* c) { return c->uploaded; }
+sr_status sr_ctx_guard(sr_ctx* c, const std::function<void()>& body) { return guarded(c, body); }
+
+extern "C" {
 
 cudaStream_t sr_ctx_stream(sr_ctx* c) { return c->stream; }
 

@@ -1791,6 +1791,23 @@ void heat_report(HeatSolver* H, cudaStream_t s, sr_heat_report* rep) {
 
 void heat_account_launches(HeatSolver* H, cudaStream_t s) { heat_sync_report(H, s); }
 
+bool heat_capturable(const HeatSolver* H) {
+    return H->precond != SR_PRECOND_LEARNED && H->use_graphs && H->mg.tuned;
+}
+
+void heat_prepare_capture(HeatSolver* H, cudaStream_t s) {
+    heat_sync_report(H, s);
+    ctl_configure(H, s);
+}
+
+long long heat_capture_step(HeatSolver* H, float* U, const float* kappa, const double* dt_dev, cudaStream_t s,
+                            cudaGraph_t root) {
+    capture_heat_step(H, U, kappa, dt_dev, s, root);
+    return H->body_launches[B_COUNT];
+}
+
+void heat_graph_launched(HeatSolver* H) { H->report_pending = true; }
+
 void heat_first_solve(HeatSolver* H, const float* U, const float* kappa, double dt, uint32_t precond, cudaStream_t s,
                       double* ms, uint32_t* rounds, double* rel_residual, double* x, uint32_t* fallback) {
     if (precond == SR_PRECOND_LEARNED && !H->lapply)

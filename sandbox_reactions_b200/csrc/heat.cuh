@@ -15,6 +15,15 @@ void heat_read_flux(HeatSolver* hs, float* fx, float* fy);
 void heat_report(HeatSolver* hs, cudaStream_t s, sr_heat_report* rep);
 // Adds the kernels the captured steps launched since the last count to the library's launch count (waits for them).
 void heat_account_launches(HeatSolver* hs, cudaStream_t s);
+// The implicit step as part of a larger captured graph (a context's whole step, a batch's): possible once the solver
+// runs under device control (MG or Jacobi, after its first step tuned the multigrid). heat_prepare_capture (outside any
+// capture) writes the control block; heat_capture_step appends the step to the capture in progress on `s` (root: the
+// graph being captured; returns its top-level kernel count); heat_graph_launched marks its report as pending.
+bool heat_capturable(const HeatSolver* hs);
+void heat_prepare_capture(HeatSolver* hs, cudaStream_t s);
+long long heat_capture_step(HeatSolver* hs, float* U, const float* kappa, const double* dt_dev, cudaStream_t s,
+                            cudaGraph_t root);
+void heat_graph_launched(HeatSolver* hs);
 // Forgets the last step's rates (a new state was uploaded).
 void heat_reset(HeatSolver* hs, cudaStream_t s);
 void heat_set_precond(HeatSolver* hs, uint32_t precond);

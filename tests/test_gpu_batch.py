@@ -34,3 +34,20 @@ def test_a_refused_world_is_named():
     good = Config(width=64, height=64)
     with pytest.raises(SrError, match="world 1"):
         Batch([good, Config(width=60, height=64)])
+
+
+def test_a_captured_step_matches_the_launched_one():
+    # after the first step (which tunes the multigrid) a context runs each whole step as one captured graph, the
+    # implicit step under device control; with timing on the passes are launched one by one: the same state either way
+    cfg, P, kappa = scenes.full_step(96, scene=5)
+    out = []
+    for timed in (False, True):
+        with Step(cfg) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            s.set_timing(timed)
+            for _ in range(3):
+                s.run(1)
+            out.append((s.readback(), s.read_heat()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert out[0][1].rounds == out[1][1].rounds and out[0][1].passes == out[1][1].passes
