@@ -6,8 +6,11 @@ One step = P1 → P2 → P4 (with its half-step gravity solve) → P5 (Newton + 
 seeded synthetic world of S x S cells (default 2048): a Gaussian disk with lognormal noise in Keplerian rotation, a
 lognormal opacity field with a 32-cell correlation length over six decades, hot spots in the gas (scenes.full_step).
 Under torchrun every rank advances its own world (scene seed = rank): the worlds are independent, no collective on the
-data path, weak scaling. The line also carries the FLD time-to-1e-8 of the 2048² implicit-diffusion configuration
-(scenes.fld) with plain MG-PCG and with Jacobi-PCG.
+data path, weak scaling. The line also carries: the FLD time-to-1e-8 of the 2048² implicit-diffusion configuration
+(scenes.fld) with plain MG-PCG, Jacobi-PCG and the learned preconditioner; the other single-GPU configurations (Sod
+512², the 1024² disk) with their parity against the oracle; the full-size parity of one step against the f64 twin;
+and config 5, 64 worlds of a seeded 256²…2048² mix advanced as one captured graph per batch step against the same
+worlds one at a time (`batched`).
 
 `--impl reference` times the reference's own CPU algorithm (the f64 twin restated in C, oracle/) on the same 2048²
 world with every host thread, for as many of the K steps as fit a bounded time (at least one), and beside it one
@@ -414,14 +417,58 @@ def config_runs(peak_gbs: float):
     return out
 
 
+def batch_measure(count: int, steps: int, warmup: int, rank: int = 0, world: int = 1, dist=None):
+    """Config 5 on this rank: its share (by cell count) of `count` worlds of a seeded 256²…2048² mix advanced as one
+    batch — after the first step each batch step is one captured CUDA graph over all of them — against the same worlds
+    stepped one at a time; device ms of the timed steps (max over ranks) and the cells. The warm-up covers the first,
+    host-driven step and the capture of the two state-buffer parities' graphs."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from sandbox_reactions_b200 import distributed, scenes
+    from sandbox_reactions_b200.engine import Batch, Step
+
+    specs = scenes.batch_mix(count, sizes=(256, 512, 1024, 2048))
+    cells = [n * n for n, _, _ in specs]
+    mine = distributed.partition(cells, world)[rank]
+    with ThreadPoolExecutor(8) as ex:  # numpy's FFTs and sorts release the GIL
+        worlds = list(ex.map(scenes.world, [specs[i] for i in mine]))
+    batch = Batch([w[0] for w in worlds])
+    for i, (cfg, P, kappa) in enumerate(worlds):
+        batch.upload(i, P, kappa)
+    for _ in range(warmup):
+        batch.run(1)
+    if dist:
+        dist.barrier()
+    ms = batch.run(steps)
+    batch.close()
+    alone = 0.0
+    for cfg, P, kappa in worlds:
+        with Step(cfg) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            for _ in range(warmup):
+                s.run(1)
+            s.set_timing(True)
+            s.run(steps)
+            alone += s.read_cost().total_ms
+    if dist:
+        ms = distributed.max_over_ranks(dist, ms, device="cuda")
+        alone = distributed.max_over_ranks(dist, alone, device="cuda")
+    total = sum(cells)
+    return {"value": total * steps / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "warmup": warmup, "worlds": count, "cells": total,
+            "sizes": {str(n): sum(1 for c in cells if c == n * n) for n in (256, 512, 1024, 2048)},
+            "one_at_a_time": {"value": total * steps / (alone / 1e3) / 1e6, "unit": UNIT,
+                              "ms_per_step": alone / steps},
+            "speedup_vs_one_at_a_time": alone / ms}
+
+
 def run_batch(args, rank, world, local):
-    """Config 5: a seeded mix of worlds split over the ranks by cell count, each rank's share advanced as one batch;
-    the aggregate Mcell-steps/s beside the same worlds stepped one at a time."""
+    """Config 5 as the benchmark: the batch's aggregate Mcell-steps/s, worlds split over the ranks by cell count."""
     import torch
 
     from sandbox_reactions_b200 import build as lib_build
-    from sandbox_reactions_b200 import distributed, scenes
-    from sandbox_reactions_b200.engine import Batch, Step
+    from sandbox_reactions_b200 import distributed
 
     torch.cuda.set_device(local)
     dist = distributed.init("nccl")
@@ -429,47 +476,17 @@ def run_batch(args, rank, world, local):
         lib_build.build()
     if dist:
         dist.barrier()
-    specs = scenes.batch_mix(args.batch, sizes=(256, 512, 1024, 2048))
-    cells = [n * n for n, _, _ in specs]
-    mine = distributed.partition(cells, world)[rank]
-    worlds = [scenes.world(specs[i]) for i in mine]
-    batch = Batch([w[0] for w in worlds])
-    for i, (cfg, P, kappa) in enumerate(worlds):
-        batch.upload(i, P, kappa)
-    for _ in range(args.warmup):
-        batch.run(1)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ms = batch.run(args.steps)
-    torch.cuda.synchronize()
-    slow = distributed.max_over_ranks(dist, ms, device="cuda")
-    batch.close()
-    # the same worlds one at a time (device time summed), on this rank
-    alone = 0.0
-    for cfg, P, kappa in worlds:
-        with Step(cfg) as s:
-            s.upload(P)
-            s.upload_opacity(kappa)
-            for _ in range(args.warmup):
-                s.run(1)
-            s.set_timing(True)
-            s.run(args.steps)
-            alone += s.read_cost().total_ms
-    alone = distributed.max_over_ranks(dist, alone, device="cuda")
-    total_cells = sum(cells)
+    out = batch_measure(args.batch, args.steps, max(args.warmup, 3), rank, world, dist)
     if rank == 0:
-        value = total_cells * args.steps / (slow / 1e3) / 1e6
-        line = {"metric": "Mcell-steps/s batched hydro+grav+FLD (config 5)", "value": value, "unit": UNIT,
-                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": slow / args.steps,
+        line = {"metric": "Mcell-steps/s batched hydro+grav+FLD (config 5)", "value": out["value"], "unit": UNIT,
+                "n_gpus": world, "steps": args.steps, "warmup": out["warmup"], "ms_per_step": out["ms_per_step"],
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
                 "config": {"workload": f"{args.batch} worlds, seeded mix of 256/512/1024/2048 square, full step "
-                                       f"hydro+gravity+FLD (MG-PCG)", "cells": total_cells,
-                           "sizes": {str(n): sum(1 for c in cells if c == n * n) for n in (256, 512, 1024, 2048)},
+                                       f"hydro+gravity+FLD (MG-PCG), one captured graph per batch step",
+                           "cells": out["cells"], "sizes": out["sizes"],
                            "parallelism": f"worlds split over {world} GPU(s) by cell count"},
-                "one_at_a_time": {"value": total_cells * args.steps / (alone / 1e3) / 1e6, "unit": UNIT,
-                                  "ms_per_step": alone / args.steps}}
+                "one_at_a_time": out["one_at_a_time"]}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -491,6 +508,7 @@ def main():
     ap.add_argument("--solves", type=int, default=3)
     ap.add_argument("--precond", default="mg")
     ap.add_argument("--no-fld", action="store_true", help="skip the FLD time-to-1e-8 measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-world batch (config 5) side measurement")
     ap.add_argument("--batch", type=int, default=0,
                     help="run config 5 instead: this many worlds of a seeded 256..2048 mix, batched vs one at a time")
     args = ap.parse_args()
@@ -593,11 +611,14 @@ def main():
         del twin
     fld = None
     configs = None
+    batched = None
     if rank == 0 and not args.no_fld and world == 1:
         step.close()
         fld = fld_time_to_tol(2048 if n >= 2048 else n)
         configs = config_runs(measured_peaks()[0])
     step.close()
+    if rank == 0 and not args.no_batch and world == 1:
+        batched = batch_measure(64, 2, 3)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -638,6 +659,7 @@ def main():
             "parity": parity,
             "fld_time_to_1e-8": fld,
             "other_configs": configs,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if dist:
