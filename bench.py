@@ -628,7 +628,7 @@ def main():
         sm_ms = pre_ms + post_ms
         achieved = sm_bytes / (sm_ms / 1e3) / 1e9 if sm_ms > 0 else None
         tr_pre, tr_post = committed_traffic("mg_smooth_pre_level0", n * n), committed_traffic("mg_smooth_post_level0", n * n)
-        roofline = {"kernel": "mg_smooth_kernel level 0 (pre + post, one V-cycle)", "bound": "hbm",
+        roofline = {"kernel": "mg_rowband_kernel level 0 (pre + post, one V-cycle)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None,
                     "traffic": (tr_pre + tr_post) if tr_pre and tr_post else None,
@@ -636,7 +636,7 @@ def main():
                     "algorithmic_bytes_per_cell": {"pre": SMOOTH_PRE_BYTES_PER_CELL,
                                                    "post": SMOOTH_POST_BYTES_PER_CELL},
                     "peak_kind": "burst copy bandwidth (kernels timed alone)",
-                    "other": {"hydro_tile_kernel<kHydroUpdateGrav>": {
+                    "other": {"hydro_band_kernel<kHydroUpdateGrav>": {
                         "achieved": upd_gbs, "frac": upd_gbs / peak, "ms_per_launch": upd_ms,
                         "algorithmic_bytes_per_cell": HYDRO_UPDATE_BYTES_PER_CELL,
                         "traffic": committed_traffic("hydro_update", n * n)}}}

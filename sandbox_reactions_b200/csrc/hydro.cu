@@ -713,15 +713,38 @@ __global__ void floors_dt_kernel(HydroConst H, float* __restrict__ U, const floa
 }
 
 // Δt_{n+1} = min(C / max rate, η_g / sqrt(max |g|)) (hydro.rs:618-634), the configured fixed Δt or cap, and the guard.
+// One CTA: each thread takes a strided share of the partials, then a shuffle and shared-memory tree (max and min are
+// exact in any order, so the result does not depend on the split).
 __global__ void dt_finalize_kernel(int nblocks, const float* part_rate, const float* part_g, const long long* part_nf,
                                    double cfl, double eta_g, double dt_fixed, double dt_cap, DtRecord* rec) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
     float rate = 0.0f, gmax = 0.0f;
     long long nf = LLONG_MAX;
-    for (int b = 0; b < nblocks; b++) {
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
         rate = fmaxf(rate, part_rate[b]);
         gmax = fmaxf(gmax, part_g[b]);
         nf = part_nf[b] < nf ? part_nf[b] : nf;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rate = fmaxf(rate, __shfl_down_sync(0xffffffffu, rate, o));
+        gmax = fmaxf(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
+        const long long on = __shfl_down_sync(0xffffffffu, nf, o);
+        nf = on < nf ? on : nf;
+    }
+    __shared__ float sr[32], sg[32];
+    __shared__ long long sn[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sr[warp] = rate;
+        sg[warp] = gmax;
+        sn[warp] = nf;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int k = 1; k < (int)(blockDim.x / 32); k++) {
+        rate = fmaxf(rate, sr[k]);
+        gmax = fmaxf(gmax, sg[k]);
+        nf = sn[k] < nf ? sn[k] : nf;
     }
     double dt = cfl / (double)rate;
     if (gmax > 0.0f) dt = fmin(dt, eta_g / sqrt((double)gmax));
@@ -756,7 +779,7 @@ void floors_dt_launch(const HydroConst& H, float* U, const float* gx, const floa
     int nb = floors_dt_blocks(H.w, H.h);
     floors_dt_kernel<<<nb, 256, 0, s>>>(H, U, gx, gy, do_floors, part_rate, part_g, part_nf);
     sr_note_launch();
-    dt_finalize_kernel<<<1, 32, 0, s>>>(nb, part_rate, part_g, part_nf, cfl, eta_g, dt_fixed, dt_cap, rec);
+    dt_finalize_kernel<<<1, 256, 0, s>>>(nb, part_rate, part_g, part_nf, cfl, eta_g, dt_fixed, dt_cap, rec);
     sr_note_launch();
 }
 
