@@ -40,6 +40,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-steps/s hydro+grav+FLD @2048²; FLD time-to-1e-8: learned vs MG-PCG"
 UNIT = "Mcell-steps/s"
+BREAKDOWN_STEPS = 2  # steps of the per-pass timing leg (passes launched one by one) after the timed steps
 # algorithmic bytes per cell of the fused hydro update kernel with gravity: state in 16 + out 16, P2's g 8,
 # the half-step source 4, φ_mid 4 and g_mid 8
 HYDRO_UPDATE_BYTES_PER_CELL = 56
@@ -255,7 +256,7 @@ def run_case(args, local):
         cfg, P = scenes.disk(n)
         with Step(cfg.replace(hydro=False, heat=False)) as s:
             s.upload(P)
-            s.set_timing(True)
+            s.set_timing(2)
             s.run(args.solves)  # each step: P2's solve, P8, P9
             cost = s.read_cost()
         print(f"grav {n}: {args.solves} solves, {cost.gravity_ms / args.solves:.3f} ms per solve")
@@ -377,17 +378,20 @@ def config_runs(peak_gbs: float):
             one = s.readback()
             dt1 = s.read_dt().dt
             s.run(2)
-            s.set_timing(True)
+            s.set_timing(1)
             s.run(steps)
             c = s.read_cost()
-            s.set_timing(False)
+            s.set_timing(2)  # a short per-pass leg for the hydro update kernel's own time
+            s.run(4)
+            cu = s.read_cost()
+            s.set_timing(0)
             if not cfg.gravity:
                 s.upload(P)
                 s.run(steps)
                 final = s.readback()
                 sim_time = s.read_dt().sim_time
         n = cfg.width * cfg.height
-        upd = c.hydro_update_ms / max(1, c.hydro_update_launches)
+        upd = cu.hydro_update_ms / max(1, cu.hydro_update_launches)
         gbs = bpc * n / (upd / 1e3) / 1e9
         P64 = P.astype(np.float64)
         g = O.grav_field(cfg, P64[0])[1:] if cfg.gravity else None
@@ -497,7 +501,7 @@ def run_batch(args, rank, world, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--size", type=int, default=2048)
     ap.add_argument("--ref-budget", type=float, default=120.0,
@@ -556,12 +560,16 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    step.set_timing(True)
+    step.set_timing(1)  # each step's device time, the steps run as they always do (one captured graph per step)
     with sampler:
         step.run(args.steps)
     torch.cuda.synchronize()
     cost = step.read_cost()
-    step.set_timing(False)
+    # a short second leg with the passes launched one by one: the per-pass breakdown and the hydro update's own time
+    step.set_timing(2)
+    step.run(BREAKDOWN_STEPS)
+    parts = step.read_cost()
+    step.set_timing(0)
     total_ms = cost.total_ms
     t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
     if dist:
@@ -622,7 +630,7 @@ def main():
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        upd_ms = cost.hydro_update_ms / max(1, cost.hydro_update_launches)
+        upd_ms = parts.hydro_update_ms / max(1, parts.hydro_update_launches)
         upd_gbs = HYDRO_UPDATE_BYTES_PER_CELL * n * n / (upd_ms / 1e3) / 1e9
         sm_bytes = (SMOOTH_PRE_BYTES_PER_CELL + SMOOTH_POST_BYTES_PER_CELL) * n * n
         sm_ms = pre_ms + post_ms
@@ -652,8 +660,12 @@ def main():
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,
-            "breakdown_ms_per_step": {"gravity": cost.gravity_ms / args.steps, "hydro": cost.hydro_ms / args.steps,
-                                      "heat": cost.heat_ms / args.steps, "floors_dt": cost.dt_ms / args.steps},
+            "breakdown_ms_per_step": {"gravity": parts.gravity_ms / BREAKDOWN_STEPS,
+                                      "hydro": parts.hydro_ms / BREAKDOWN_STEPS,
+                                      "heat": parts.heat_ms / BREAKDOWN_STEPS,
+                                      "floors_dt": parts.dt_ms / BREAKDOWN_STEPS,
+                                      "total": parts.total_ms / BREAKDOWN_STEPS,
+                                      "how": f"{BREAKDOWN_STEPS} further steps with the passes launched one by one"},
             "heat_last_step": {"passes": heat.passes, "rounds": heat.rounds, "refinements": heat.refinements,
                                "converged": heat.converged, "rel_residual": heat.rel_residual},
             "parity": parity,

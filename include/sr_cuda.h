@@ -181,7 +181,9 @@ sr_status sr_set_edge_mode(sr_ctx* ctx, uint32_t edge);
 sr_status sr_set_heat_precond(sr_ctx* ctx, uint32_t precond);
 /* Step::set_heat_rounds (step/heat.rs:529-533): the ceilings of the implicit step. */
 sr_status sr_set_heat_limits(sr_ctx* ctx, uint32_t max_passes, uint32_t max_rounds);
-/* Step::set_timing / read_cost (step/mod.rs:722-777). */
+/* Step::set_timing / read_cost (step/mod.rs:722-777). `on`: 0 off; 1 each step's device time (total_ms) as the steps
+ * normally run — after the first step, one captured graph per step — with the per-pass fields left 0; 2 the per-pass
+ * breakdown, the passes launched one by one (the implicit step still one captured graph after the first step). */
 sr_status sr_set_timing(sr_ctx* ctx, int32_t on);
 sr_status sr_read_cost(sr_ctx* ctx, sr_cost* out);
 

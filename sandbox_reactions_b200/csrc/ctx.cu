@@ -60,7 +60,7 @@ struct sr_ctx {
     long long step_launches = 0;
     unsigned generation = 0;  // counts the invalidations of captured steps (a batch's graph checks it)
     // timing
-    bool timing = false;
+    int timing = 0;  // 0 off; 1 each step's device time (captured steps); 2 per pass (passes launched one by one)
     std::vector<cudaEvent_t> events;
     sr_cost cost{};
     std::string error;
@@ -283,39 +283,53 @@ void sr_ctx_graph_steps_done(sr_ctx* c, uint32_t steps, long long launches_per_s
     sr_note_launches(launches_per_step * (long long)steps);
 }
 
+// Captures the whole step from the current state buffer as a graph (once per buffer).
+static void capture_step_graph(sr_ctx* c) {
+    sr_ctx_prepare_capture(c);
+    cudaGraph_t g;
+    SR_CUDA_TRY(cudaGraphCreate(&g, 0));
+    SR_CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    long long n = 0;
+    try {
+        n = sr_ctx_capture_step(c, c->cur, c->stream, g);
+    } catch (...) {
+        cudaGraph_t dead;
+        cudaStreamEndCapture(c->stream, &dead);
+        cudaGraphDestroy(g);
+        throw;
+    }
+    cudaGraph_t out;
+    SR_CUDA_TRY(cudaStreamEndCapture(c->stream, &out));
+    const cudaError_t e = cudaGraphInstantiate(&c->step_graph[c->cur], g, 0);
+    cudaGraphDestroy(g);
+    SR_CUDA_TRY(e);
+    c->step_launches = n;
+}
+
 static void run_steps(sr_ctx* c, uint32_t steps) {
     const unsigned long long launches0 = sr_launches();
-    // without timing, after the first step (which tunes the multigrid), every step is one captured graph
-    if (!c->timing && steps && capturable(c)) {
-        if (!c->step_graph[c->cur]) {
-            sr_ctx_prepare_capture(c);
-            cudaGraph_t g;
-            SR_CUDA_TRY(cudaGraphCreate(&g, 0));
-            SR_CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-            long long n = 0;
-            try {
-                n = sr_ctx_capture_step(c, c->cur, c->stream, g);
-            } catch (...) {
-                cudaGraph_t dead;
-                cudaStreamEndCapture(c->stream, &dead);
-                cudaGraphDestroy(g);
-                throw;
-            }
-            cudaGraph_t out;
-            SR_CUDA_TRY(cudaStreamEndCapture(c->stream, &out));
-            const cudaError_t e = cudaGraphInstantiate(&c->step_graph[c->cur], g, 0);
-            cudaGraphDestroy(g);
-            SR_CUDA_TRY(e);
-            c->step_launches = n;
-        }
+    // after the first step (which tunes the multigrid) every step is one captured graph, unless the per-pass timing
+    // (2) asks for the passes launched one by one; timing 1 records the device time of each step's graph
+    if (c->timing != 2 && steps && capturable(c)) {
         for (uint32_t s = 0; s < steps; s++) {
-            if (!c->step_graph[c->cur]) break;
+            if (!c->step_graph[c->cur]) capture_step_graph(c);  // before the step's start event
+            if (c->timing) SR_CUDA_TRY(cudaEventRecord(event_at(c, 2 * (size_t)s), c->stream));
             SR_CUDA_TRY(cudaGraphLaunch(c->step_graph[c->cur], c->stream));
+            if (c->timing) SR_CUDA_TRY(cudaEventRecord(event_at(c, 2 * (size_t)s + 1), c->stream));
             sr_ctx_graph_steps_done(c, 1, c->step_launches);
-            if (!c->step_graph[c->cur] && s + 1 < steps) {  // the other state buffer's graph, captured on first use
-                run_steps(c, steps - s - 1);
-                return;
+        }
+        if (c->timing) {
+            SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+            if (c->heat) heat_account_launches(c->heat, c->stream);
+            sr_cost& t = c->cost;
+            memset(&t, 0, sizeof t);
+            t.steps = steps;
+            for (uint32_t s = 0; s < steps; s++) {
+                float ms = 0.0f;
+                SR_CUDA_TRY(cudaEventElapsedTime(&ms, c->events[2 * (size_t)s], c->events[2 * (size_t)s + 1]));
+                t.total_ms += ms;
             }
+            t.kernel_launches = sr_launches() - launches0;
         }
         return;
     }
@@ -592,7 +606,7 @@ sr_status sr_set_heat_limits(sr_ctx* c, uint32_t max_passes, uint32_t max_rounds
 }
 
 sr_status sr_set_timing(sr_ctx* c, int32_t on) {
-    return guarded(c, [&] { c->timing = on != 0; });
+    return guarded(c, [&] { c->timing = on <= 0 ? 0 : (on == 1 ? 1 : 2); });
 }
 
 sr_status sr_read_cost(sr_ctx* c, sr_cost* out) {

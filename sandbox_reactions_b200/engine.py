@@ -205,8 +205,10 @@ class Step:
     def set_heat_limits(self, max_passes: int, max_rounds: int):
         self._check(self.lib.sr_set_heat_limits(self._h, max_passes, max_rounds))
 
-    def set_timing(self, on: bool = True):
-        self._check(self.lib.sr_set_timing(self._h, int(on)))
+    def set_timing(self, level: int = 1):
+        """0 off; 1 (or True) each step's device time, the steps run as they normally do (one captured graph per
+        step after the first); 2 the per-pass breakdown, the passes launched one by one."""
+        self._check(self.lib.sr_set_timing(self._h, int(level)))
 
     def read_cost(self) -> sr_cost:
         r = sr_cost()
