@@ -11,7 +11,7 @@
 use std::ffi::CStr;
 use std::os::raw::{c_char, c_void};
 
-pub const SR_ABI_VERSION: u32 = 2;
+pub const SR_ABI_VERSION: u32 = 3;
 
 pub type sr_status = i32;
 pub const SR_OK: sr_status = 0;
@@ -77,6 +77,16 @@ pub struct sr_config {
     pub mg_omega: f64,
     pub inner_tol: f64,
     pub reserved_d: [f64; 2],
+    pub k1e: f64,
+    pub k2e: f64,
+    pub k1n: f64,
+    pub k2n: f64,
+    pub kappa_dust: f64,
+    pub t_dust: f64,
+    pub sigma_hold: f64,
+    pub eta_hold: f64,
+    pub r_hold: f64,
+    pub m_tov: f64,
 }
 
 #[repr(C)]
@@ -143,6 +153,8 @@ extern "C" {
     pub fn sr_destroy(ctx: *mut sr_ctx);
     pub fn sr_upload(ctx: *mut sr_ctx, planes: *const f32, nplanes: u32) -> sr_status;
     pub fn sr_readback(ctx: *mut sr_ctx, planes: *mut f32, nplanes: u32) -> sr_status;
+    pub fn sr_upload_held(ctx: *mut sr_ctx, mask: *const u32) -> sr_status;
+    pub fn sr_read_held(ctx: *mut sr_ctx, mask: *mut u32) -> sr_status;
     pub fn sr_upload_opacity(ctx: *mut sr_ctx, kappa: *const f32) -> sr_status;
     pub fn sr_step(ctx: *mut sr_ctx, steps: u32) -> sr_status;
     pub fn sr_read_dt(ctx: *mut sr_ctx, out: *mut sr_dt_report) -> sr_status;
@@ -235,10 +247,23 @@ impl Step {
         self.cfg.width as usize * self.cfg.height as usize
     }
 
-    /// `State::upload` (state.rs:251): the 4 canonical channel-major f32 planes.
+    /// `State::upload` (state.rs:251): the context's canonical channel-major f32 planes (4, or 14 in reference mode).
     pub fn upload(&mut self, planes: &[f32]) -> Result<(), Error> {
-        assert_eq!(planes.len(), 4 * self.plane_len(), "4 planes of width x height");
-        self.check(unsafe { sr_upload(self.ctx, planes.as_ptr(), 4) })
+        let nc = self.cfg.channels as usize;
+        assert_eq!(planes.len(), nc * self.plane_len(), "one plane of width x height per channel");
+        self.check(unsafe { sr_upload(self.ctx, planes.as_ptr(), nc as u32) })
+    }
+
+    /// `State::upload_held` (state.rs:198-211): the hold's mask, one word per cell (reference mode).
+    pub fn upload_held(&mut self, mask: &[u32]) -> Result<(), Error> {
+        assert_eq!(mask.len(), self.plane_len(), "one word per cell");
+        self.check(unsafe { sr_upload_held(self.ctx, mask.as_ptr()) })
+    }
+
+    /// `State::read_held` (state.rs:213-250).
+    pub fn read_held(&mut self, mask: &mut [u32]) -> Result<(), Error> {
+        assert_eq!(mask.len(), self.plane_len(), "one word per cell");
+        self.check(unsafe { sr_read_held(self.ctx, mask.as_mut_ptr()) })
     }
 
     pub fn upload_opacity(&mut self, kappa: &[f32]) -> Result<(), Error> {
@@ -253,8 +278,9 @@ impl Step {
 
     /// `State::readback` (state.rs:273).
     pub fn readback(&mut self, planes: &mut [f32]) -> Result<(), Error> {
-        assert_eq!(planes.len(), 4 * self.plane_len(), "4 planes of width x height");
-        self.check(unsafe { sr_readback(self.ctx, planes.as_mut_ptr(), 4) })
+        let nc = self.cfg.channels as usize;
+        assert_eq!(planes.len(), nc * self.plane_len(), "one plane of width x height per channel");
+        self.check(unsafe { sr_readback(self.ctx, planes.as_mut_ptr(), nc as u32) })
     }
 
     /// `Step::read_dt` (step/dt.rs:173).

@@ -7,8 +7,8 @@
  *
  * Conventions (the reference's canonical layout, crates/sr-engine/src/state.rs:1-38):
  *   - planes are f32, channel-major, row-major inside a plane: value (c, x, y) at c*W*H + y*W + x, y down;
- *   - channels: 0 Σ (surface density), 1 Σu, 2 Σv, 3 E (energy per area), then species mass fractions when the
- *     reference EOS carries them (not in this build: `channels` is 4);
+ *   - channels: 0 Σ (surface density), 1 Σu, 2 Σv, 3 E (energy per area), then, with `channels` 14 (reference mode),
+ *     the ten species' mass fractions X_H, X_He, X_C, X_O, X_Ne, X_Mg, X_Si, X_S, X_Fe, X_n (state.rs:29-35);
  *   - x faces: (W+1)*H values, face (x, y) between cells (x-1, y) and (x, y); y faces: W*(H+1) values, face (x, y)
  *     between (x, y-1) and (x, y); a flux is positive toward +x / +y (crates/sr-physics/src/reference/heat.rs:94-101).
  *
@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define SR_ABI_VERSION 2u
+#define SR_ABI_VERSION 3u
 
 typedef enum sr_status {
     SR_OK = 0,
@@ -58,7 +58,9 @@ enum { SR_PRECOND_MG = 0, SR_PRECOND_JACOBI = 1, SR_PRECOND_LEARNED = 2 };
 typedef struct sr_config {
     uint32_t struct_size;     /* sizeof(sr_config): guards against a header/library mismatch */
     uint32_t width, height;   /* multiples of 8, 8..4096 */
-    uint32_t channels;        /* 4: Σ, Σu, Σv, E */
+    uint32_t channels;        /* 4: Σ, Σu, Σv, E under the config-mode EOS (γ, μ); 14: reference mode — the reference's
+                                 own EOS (γ = 2, μ and Y_e of each cell's species, the cold pressures of the K pairs),
+                                 species advected, the hold (held cells behind reflecting walls) */
     uint32_t edge;            /* SR_EDGE_* */
     uint32_t limiter;         /* SR_LIMITER_* */
     uint32_t thermal_bracket; /* 1: the reference's HOT_FACE bracket on Σ and Π slopes (hydro.rs:310-331) */
@@ -97,6 +99,12 @@ typedef struct sr_config {
     double mg_omega;          /* weight of the multigrid's coarse correction (0: the library's default) */
     double inner_tol;         /* smallest residual reduction asked of one FP32 inner solve (0: default 1e-5) */
     double reserved_d[2];
+    /* reference mode (channels 14): physics.json's constants the 4-channel field update does not read */
+    double k1e, k2e;          /* the electrons' cold-pressure pair K₁, K₂; both 0: off (eos.rs:150-190) */
+    double k1n, k2n;          /* neutron matter's pair */
+    double kappa_dust, t_dust; /* the dust opacity stand-in of the radiation force (reference/hydro.rs:365-382) */
+    double sigma_hold, eta_hold, r_hold; /* the hold's Σ, ε_th/ε_cold and gate radius (reference/floors.rs:94-110) */
+    double m_tov;             /* m_tov_sb: the hold's disk-mass gate (floors.rs:90-92; assets/calibration.json) */
 } sr_config;
 
 /* Δt record (crates/sr-engine/src/step/dt.rs:51-61). */
@@ -159,6 +167,11 @@ void sr_destroy(sr_ctx* ctx);
 sr_status sr_upload(sr_ctx* ctx, const float* planes, uint32_t nplanes);
 /* State::readback (state.rs:273). */
 sr_status sr_readback(sr_ctx* ctx, float* planes, uint32_t nplanes);
+/* State::upload_held / read_held (crates/sr-engine/src/state.rs:198-250): the hold's mask, one word per cell, row-major,
+ * nonzero where a cell is held — reference mode only (channels 14). sr_upload clears the mask and applies the hold's
+ * rule to the new state (reference/mod.rs:129-177); sr_upload_held then replaces the mask (a dump's, resumed). */
+sr_status sr_upload_held(sr_ctx* ctx, const uint32_t* mask);
+sr_status sr_read_held(sr_ctx* ctx, uint32_t* mask);
 /* The opacity plane κ (W*H f32) read when cfg.opacity_plane is 1. */
 sr_status sr_upload_opacity(sr_ctx* ctx, const float* kappa);
 

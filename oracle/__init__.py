@@ -24,6 +24,11 @@ class or_hydro_report(C.Structure):
     _fields_ = [("kick_net", C.c_double * 2), ("densest", C.c_int64), ("escaped", C.c_double * 4)]
 
 
+class or_ref_hydro_report(C.Structure):
+    _fields_ = [("spared", C.c_double * 2), ("kick_net", C.c_double * 2), ("densest", C.c_int64),
+                ("push_net", C.c_double * 2), ("push_abs", C.c_double)]
+
+
 class or_heat_report(C.Structure):
     _fields_ = [("passes", C.c_int64), ("rounds", C.c_int64), ("delta", C.c_double), ("converged", C.c_int32),
                 ("pad", C.c_int32), ("radiated", C.c_double)]
@@ -31,7 +36,8 @@ class or_heat_report(C.Structure):
 
 def build() -> str:
     """Compiles the oracle (gcc, OpenMP) when its library is missing or older than its sources."""
-    src = [os.path.join(HERE, f) for f in ("sr_oracle.c", "sr_oracle.h", "Makefile")]
+    src = [os.path.join(HERE, f) for f in ("sr_oracle.c", "sr_oracle_ref.c", "sr_oracle.h", "Makefile",
+                                           os.path.join("..", "include", "sr_cuda.h"))]
     if not os.path.exists(LIB_PATH) or max(os.path.getmtime(s) for s in src) > os.path.getmtime(LIB_PATH):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
@@ -79,6 +85,31 @@ def lib():
         L.or_twin_clock.argtypes = [C.c_void_p, _D]
         L.or_twin_field.argtypes = [C.c_void_p, _D, _D, _D]
         L.or_twin_heat.argtypes = [C.c_void_p, C.POINTER(or_heat_report), _D, _D]
+        U8 = C.POINTER(C.c_uint8)
+        L.or_cold_pressure.restype = C.c_double
+        L.or_cold_pressure.argtypes = [C.c_double] * 3
+        L.or_cold_energy_exact.restype = C.c_double
+        L.or_cold_energy_exact.argtypes = [C.c_double] * 3
+        L.or_cold_table.argtypes = [C.c_double, C.c_double, _D]
+        L.or_cold_table_u.restype = C.c_double
+        L.or_cold_table_u.argtypes = [_D, C.c_double]
+        L.or_composition.argtypes = [_D, _D]
+        L.or_ref_hydro_step.argtypes = [P, _D, C.c_int64, C.c_int64, C.c_double, _D, _D, U8, _D, _D,
+                                        C.POINTER(or_ref_hydro_report)]
+        L.or_ref_dt.restype = C.c_double
+        L.or_ref_dt.argtypes = [P, _D, C.c_int64, C.c_int64, _D, _D]
+        L.or_ref_floors.argtypes = [P, _D, C.c_int64, C.c_int64, _D]
+        L.or_ref_disk_mass.restype = C.c_double
+        L.or_ref_disk_mass.argtypes = [_D, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_double]
+        L.or_ref_hold.argtypes = [P, _D, C.c_int64, C.c_int64, U8, _D]
+        L.or_ref_twin_new.restype = C.c_void_p
+        L.or_ref_twin_new.argtypes = [P, _D, U8]
+        L.or_ref_twin_free.argtypes = [C.c_void_p]
+        L.or_ref_twin_set_flux.argtypes = [C.c_void_p, _D, _D]
+        L.or_ref_twin_step.argtypes = [C.c_void_p]
+        L.or_ref_twin_state.argtypes = [C.c_void_p, _D, U8]
+        L.or_ref_twin_clock.argtypes = [C.c_void_p, _D]
+        L.or_ref_twin_books.argtypes = [C.c_void_p, _D]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_get_threads.restype = C.c_int
         _lib = L
@@ -322,3 +353,130 @@ class Twin:
         fx, fy = np.zeros((h, w + 1)), np.zeros((h + 1, w))
         lib().or_twin_heat(self._t, C.byref(rep), _p(fx), _p(fy))
         return rep, fx, fy
+
+
+# ---------------------------------------------------------------- reference mode (14 channels)
+def _u8(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+def _pu8(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint8))
+
+
+def cold_pressure(x: float, k1: float, k2: float) -> float:
+    return lib().or_cold_pressure(x, k1, k2)
+
+
+def cold_energy_exact(x: float, k1: float, k2: float) -> float:
+    return lib().or_cold_energy_exact(x, k1, k2)
+
+
+def cold_table(k1: float, k2: float) -> np.ndarray:
+    """ln u at the 512 nodes (eos.rs:81-98)."""
+    out = np.zeros(512)
+    lib().or_cold_table(k1, k2, _p(out))
+    return out
+
+
+def cold_table_u(ln_u: np.ndarray, x: float) -> float:
+    return lib().or_cold_table_u(_p(_f64(ln_u)), x)
+
+
+def composition(x) -> tuple[float, float, float]:
+    out = np.zeros(3)
+    lib().or_composition(_p(_f64(x)), _p(out))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+def ref_hydro_step(cfg: Config, planes: np.ndarray, dt: float, g=None, held=None, rad=None):
+    """One reference-mode P4 step on (14, H, W) f64 planes (step_held): `g` = (gx, gy) of the start state, `held` the
+    hold's (H, W) mask, `rad` = (Fx, Fy) cell-centred for the radiation force. Returns (planes, report)."""
+    p = _f64(planes).copy()
+    _, h, w = p.shape
+    rep = or_ref_hydro_report()
+    c = cfg.to_c()
+    gx, gy = (_f64(g[0]), _f64(g[1])) if g is not None else (None, None)
+    m = _u8(held) if held is not None else None
+    rx, ry = (_f64(rad[0]), _f64(rad[1])) if rad is not None else (None, None)
+    lib().or_ref_hydro_step(C.byref(c), _p(p), w, h, dt, _p(gx) if gx is not None else None,
+                            _p(gy) if gy is not None else None, _pu8(m) if m is not None else None,
+                            _p(rx) if rx is not None else None, _p(ry) if ry is not None else None, C.byref(rep))
+    return p, rep
+
+
+def ref_dt(cfg: Config, planes: np.ndarray, g=None) -> float:
+    p = _f64(planes)
+    _, h, w = p.shape
+    c = cfg.to_c()
+    if g is None:
+        return lib().or_ref_dt(C.byref(c), _p(p), w, h, None, None)
+    return lib().or_ref_dt(C.byref(c), _p(p), w, h, _p(_f64(g[0])), _p(_f64(g[1])))
+
+
+def ref_floors(cfg: Config, planes: np.ndarray):
+    """P8's floors on (14, H, W) planes; returns (planes, (vacuum_reset, floor_added))."""
+    p = _f64(planes).copy()
+    _, h, w = p.shape
+    booked = np.zeros(2)
+    c = cfg.to_c()
+    lib().or_ref_floors(C.byref(c), _p(p), w, h, _p(booked))
+    return p, (float(booked[0]), float(booked[1]))
+
+
+def ref_hold(cfg: Config, planes: np.ndarray, held=None):
+    """The hold after P8: returns (planes with newly held momenta zeroed, mask, taken momentum)."""
+    p = _f64(planes).copy()
+    _, h, w = p.shape
+    m = np.zeros((h, w), np.uint8) if held is None else _u8(held).copy()
+    taken = np.zeros(2)
+    c = cfg.to_c()
+    lib().or_ref_hold(C.byref(c), _p(p), w, h, _pu8(m), _p(taken))
+    return p, m, (float(taken[0]), float(taken[1]))
+
+
+def disk_mass(sigma: np.ndarray, x: int, y: int, r: float) -> float:
+    s = _f64(sigma)
+    h, w = s.shape
+    return lib().or_ref_disk_mass(_p(s), w, h, x, y, r)
+
+
+class RefTwin:
+    """The reference-mode twin (reference/mod.rs:129-297 without P5) on 14 f64 planes: the hold's rule on the initial
+    state, then per step P1, P2, P4 (step_held), P8 and the hold, P9."""
+
+    def __init__(self, cfg: Config, planes: np.ndarray, mask=None):
+        self.cfg = cfg
+        self._c = cfg.to_c()
+        p = _f64(planes)
+        m = _u8(mask) if mask is not None else None
+        self._t = lib().or_ref_twin_new(C.byref(self._c), _p(p), _pu8(m) if m is not None else None)
+
+    def __del__(self):
+        if getattr(self, "_t", None):
+            lib().or_ref_twin_free(self._t)
+            self._t = None
+
+    def set_flux(self, fx: np.ndarray, fy: np.ndarray):
+        lib().or_ref_twin_set_flux(self._t, _p(_f64(fx)), _p(_f64(fy)))
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            lib().or_ref_twin_step(self._t)
+
+    def state(self):
+        h, w = self.cfg.height, self.cfg.width
+        out = np.zeros((14, h, w))
+        m = np.zeros((h, w), np.uint8)
+        lib().or_ref_twin_state(self._t, _p(out), _pu8(m))
+        return out, m
+
+    def clock(self):
+        out = np.zeros(4)
+        lib().or_ref_twin_clock(self._t, _p(out))
+        return {"dt": out[0], "dt_next": out[1], "sim_time": out[2], "steps": int(out[3])}
+
+    def books(self):
+        out = np.zeros(4)
+        lib().or_ref_twin_books(self._t, _p(out))
+        return {"held": (out[0], out[1]), "vacuum_reset": out[2], "floor_added": out[3]}

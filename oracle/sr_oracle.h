@@ -108,6 +108,48 @@ void or_twin_heat(const or_twin* t, or_heat_report* rep, double* fx, double* fy)
 void or_set_threads(int n);
 int or_get_threads(void);
 
+/* ---- Reference mode (sr_oracle_ref.c): 14 channels, the reference's own EOS, species and the hold ---- */
+/* The cold pressure P(x; K₁, K₂) (eos.rs:22-29), its energy per area in closed form (eos.rs:49-65), the 512-node
+ * table of ln u (eos.rs:81-98) and the table's u(x) (eos.rs:118-131). */
+double or_cold_pressure(double x, double k1, double k2);
+double or_cold_energy_exact(double x, double k1, double k2);
+void or_cold_table(double k1, double k2, double* ln_u);
+double or_cold_table_u(const double* ln_u, double x);
+/* 1/μ, Y_e, Z_met of ten mass fractions (registry.rs:145-154). */
+void or_composition(const double* x, double* out3);
+typedef struct or_ref_hydro_report {
+    double spared[2];   /* momentum booked `held`: the held cells' spared impulses and the sticky walls' stops */
+    double kick_net[2]; /* gravity's net kick on the gas's own field, taken back at the densest free cell */
+    int64_t densest;
+    double push_net[2]; /* the radiation force's net push, taken back */
+    double push_abs;    /* Σ |push| */
+} or_ref_hydro_report;
+/* One P4 step in place on 14 f64 planes (hydro.rs:657-1025, step_held): `gx`/`gy` P2's field of the start state or
+ * NULL; `held` the hold's mask or NULL; `radx`/`rady` the cell-centred flux of the radiation force or NULL. */
+void or_ref_hydro_step(const sr_config* cfg, double* planes, int64_t w, int64_t h, double dt, const double* gx,
+                       const double* gy, const uint8_t* held, const double* radx, const double* rady,
+                       or_ref_hydro_report* rep);
+/* Δt of a 14-channel state (hydro.rs:618-634). */
+double or_ref_dt(const sr_config* cfg, const double* planes, int64_t w, int64_t h, const double* gx,
+                 const double* gy);
+/* P8's floors (floors.rs:124-175); booked2 = [vacuum_reset, floor_added]. */
+void or_ref_floors(const sr_config* cfg, double* planes, int64_t w, int64_t h, double* booked2);
+/* The mass of the disk r about (x, y) (sinks.rs:117-125). */
+double or_ref_disk_mass(const double* sigma, int64_t w, int64_t h, int64_t x, int64_t y, double r);
+/* The hold (floors.rs:196-243): `held` in/out; taken2 = the newly held cells' momentum. */
+void or_ref_hold(const sr_config* cfg, double* planes, int64_t w, int64_t h, uint8_t* held, double* taken2);
+/* The reference-mode twin (mod.rs:129-297 without P5): P1, P2, P4, P8 + hold, P9. `mask`: the initial hold or NULL. */
+typedef struct or_ref_twin or_ref_twin;
+or_ref_twin* or_ref_twin_new(const sr_config* cfg, const double* planes, const uint8_t* mask);
+void or_ref_twin_free(or_ref_twin* t);
+void or_ref_twin_set_flux(or_ref_twin* t, const double* fx, const double* fy);
+void or_ref_twin_step(or_ref_twin* t);
+void or_ref_twin_state(const or_ref_twin* t, double* planes, uint8_t* mask);
+/* [dt, dt_next, sim_time, steps] */
+void or_ref_twin_clock(const or_ref_twin* t, double* out4);
+/* [held x, held y, vacuum_reset, floor_added] booked since the twin was made */
+void or_ref_twin_books(const or_ref_twin* t, double* out4);
+
 #ifdef __cplusplus
 }
 #endif

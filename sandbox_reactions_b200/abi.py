@@ -34,6 +34,9 @@ class sr_config(C.Structure):
         ("k_cond", C.c_double), ("chi", C.c_double), ("solve_tol", C.c_double), ("newton_heat", C.c_double),
         ("newton_cell", C.c_double), ("dt_fixed", C.c_double), ("dt_cap", C.c_double),
         ("mg_omega", C.c_double), ("inner_tol", C.c_double), ("reserved_d", C.c_double * 2),
+        ("k1e", C.c_double), ("k2e", C.c_double), ("k1n", C.c_double), ("k2n", C.c_double),
+        ("kappa_dust", C.c_double), ("t_dust", C.c_double), ("sigma_hold", C.c_double), ("eta_hold", C.c_double),
+        ("r_hold", C.c_double), ("m_tov", C.c_double),
     ]
 
 
@@ -60,6 +63,7 @@ class Config:
     """A run's configuration (the scene's world and switches, the scheme, physics.json's constants)."""
     width: int = 64
     height: int = 64
+    channels: int = 4           # 14: reference mode (the reference's EOS with species and cold pressures, the hold)
     edge: str = "bounce"
     limiter: str = "mc"
     thermal_bracket: bool = True
@@ -96,11 +100,22 @@ class Config:
     dt_cap: float = 0.0
     mg_omega: float = 0.0
     inner_tol: float = 0.0
+    # reference mode only (channels 14): physics.json's cold pairs, dust stand-in and hold, and m_tov_sb
+    # (assets/calibration.json)
+    k1e: float = 21.3
+    k2e: float = 134.0
+    k1n: float = 2.67
+    k2n: float = 58.2
+    kappa_dust: float = 0.0
+    t_dust: float = 0.0
+    sigma_hold: float = 10.0
+    eta_hold: float = 0.1
+    r_hold: float = 24.0
+    m_tov: float = 4853.169981814195
 
     def to_c(self) -> sr_config:
         c = sr_config()
         c.struct_size = C.sizeof(sr_config)
-        c.channels = 4
         enums = {"edge": EDGE, "limiter": LIMITER, "kernel": KERNEL, "precond": PRECOND}
         for f in fields(self):
             v = getattr(self, f.name)

@@ -12,6 +12,7 @@
 #include "grav.cuh"
 #include "heat.cuh"
 #include "hydro.cuh"
+#include "hydro_ref.cuh"
 #include "learned.cuh"
 
 #include <atomic>
@@ -42,6 +43,17 @@ struct sr_ctx {
     float *phi = nullptr, *gx = nullptr, *gy = nullptr;             // P2's field of the step's start state
     float *src = nullptr, *phim = nullptr, *gxm = nullptr, *gym = nullptr;  // the half step's source and field
     float* kappa = nullptr;
+    // reference mode (14 channels)
+    int nc = 4;                   // channels of the state
+    RefConst R{};
+    float* table = nullptr;       // the cold pressures' u(x) tables
+    uint8_t* held = nullptr;      // the hold's mask
+    float *src_free = nullptr, *phip = nullptr, *gxp = nullptr, *gyp = nullptr;  // the pull on the held cells
+    float* push = nullptr;        // each cell's radiation push
+    double* rpart = nullptr;      // the reference-mode P4's per-CTA partials and their reduction
+    float* rbest = nullptr;
+    int* ridx = nullptr;
+    double* rfin = nullptr;
     GravPlan grav;
     bool grav_ready = false;
     double* part_d = nullptr;
@@ -72,7 +84,15 @@ static void validate(const sr_config& c) {
                "world width must be a multiple of 8 in 16..4096 (got " + std::to_string(c.width) + ")");
     SR_REQUIRE(c.height >= 16 && c.height <= 4096 && c.height % 8 == 0,
                "world height must be a multiple of 8 in 16..4096 (got " + std::to_string(c.height) + ")");
-    SR_REQUIRE(c.channels == 4, "this build carries 4 channels (Σ, Σu, Σv, E)");
+    SR_REQUIRE(c.channels == 4 || c.channels == kRefChannels,
+               "channels must be 4 (Σ, Σu, Σv, E) or 14 (reference mode: the ten mass fractions after them)");
+    if (c.channels == kRefChannels) {
+        SR_REQUIRE(!c.heat, "reference mode (14 channels) steps P4, P2, P8 and P9; its P5 is not built: heat must be off");
+        SR_REQUIRE(c.k1e >= 0.0 && c.k2e >= 0.0 && c.k1n >= 0.0 && c.k2n >= 0.0, "the cold pairs' K must be >= 0");
+        SR_REQUIRE((c.k1e > 0.0) == (c.k2e > 0.0) && (c.k1n > 0.0) == (c.k2n > 0.0),
+                   "a cold pair is on or off as a whole (k1e/k2e, k1n/k2n)");
+        SR_REQUIRE(c.r_hold >= 0.0 && c.r_hold <= 64.0, "r_hold must be in 0..64 cells");
+    }
     SR_REQUIRE(c.edge <= SR_EDGE_LEAVE, "unknown edge mode");
     SR_REQUIRE(c.limiter <= SR_LIMITER_MINMOD, "unknown limiter");
     SR_REQUIRE(c.kernel <= SR_KERNEL_SOFTENED, "unknown gravity kernel");
@@ -126,6 +146,8 @@ static void ctx_free(sr_ctx* c) {
     cudaFree(c->phi); cudaFree(c->gx); cudaFree(c->gy);
     cudaFree(c->src); cudaFree(c->phim); cudaFree(c->gxm); cudaFree(c->gym);
     cudaFree(c->kappa);
+    cudaFree(c->table); cudaFree(c->held); cudaFree(c->src_free); cudaFree(c->phip); cudaFree(c->gxp);
+    cudaFree(c->gyp); cudaFree(c->push); cudaFree(c->rpart); cudaFree(c->rbest); cudaFree(c->ridx); cudaFree(c->rfin);
     if (c->grav_ready) c->grav.destroy();
     cudaFree(c->part_d); cudaFree(c->part_best); cudaFree(c->part_idx); cudaFree(c->hreport); cudaFree(c->herr);
     cudaFree(c->rec); cudaFree(c->part_rate); cudaFree(c->part_g); cudaFree(c->part_nf);
@@ -169,13 +191,99 @@ static sr_status guarded_free(F body) {
 
 static float* planes(sr_ctx* c) { return c->U[c->cur]; }
 
+static bool ref_mode(const sr_ctx* c) { return c->nc == kRefChannels; }
+
+// Reference mode's constants, tables and buffers.
+static void ref_setup(sr_ctx* c) {
+    const sr_config& k = c->cfg;
+    const size_t n = c->n;
+    RefConst& R = c->R;
+    R.w = c->w;
+    R.h = c->h;
+    R.edge = (int)k.edge;
+    R.limiter = (int)k.limiter;
+    R.bracket = (int)k.thermal_bracket;
+    R.cold_e = k.k1e > 0.0 && k.k2e > 0.0;
+    R.cold_n = k.k1n > 0.0 && k.k2n > 0.0;
+    R.k1e = (float)k.k1e;
+    R.k1e_k2e = R.cold_e ? (float)(k.k1e / k.k2e) : 0.0f;
+    R.k1n = (float)k.k1n;
+    R.k1n_k2n = R.cold_n ? (float)(k.k1n / k.k2n) : 0.0f;
+    R.sigma_vac = (float)k.sigma_vac;
+    R.sigma_floor = (float)k.sigma_floor;
+    R.t_floor = (float)k.t_floor;
+    R.kappa0 = (float)k.kappa0;
+    R.inv_c_sb = (float)(1.0 / k.c_sb);
+    R.kappa_dust = (float)k.kappa_dust;
+    R.t_dust = (float)k.t_dust;
+    R.sigma_hold = (float)k.sigma_hold;
+    R.eta_hold = (float)k.eta_hold;
+    R.r_hold = (float)k.r_hold;
+    R.m_tov = (float)k.m_tov;
+    std::vector<float> tab(4 * kColdPoints);
+    ref_cold_tables(k, tab.data());
+    dalloc(&c->table, tab.size());
+    SR_CUDA_TRY(cudaMemcpy(c->table, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+    R.table = c->table;
+    dalloc(&c->held, n);
+    dalloc(&c->push, 2 * n);
+    if (k.gravity) {
+        dalloc(&c->src_free, n);
+        dalloc(&c->phip, n);
+        dalloc(&c->gxp, n);
+        dalloc(&c->gyp, n);
+    }
+    const int rb = ref_hydro_blocks(c->w, c->h);
+    dalloc(&c->rpart, (size_t)rb * 5);
+    dalloc(&c->rbest, (size_t)rb);
+    dalloc(&c->ridx, (size_t)rb);
+    dalloc(&c->rfin, 6);
+}
+
+static RefArgs ref_args(sr_ctx* c, int cur) {
+    RefArgs A{};
+    A.R = c->R;
+    A.dt = &c->rec->dt;
+    A.U = c->U[cur];
+    A.Uout = c->U[1 - cur];
+    A.held = c->held;
+    A.gx = c->cfg.gravity ? c->gx : nullptr;
+    A.gy = c->cfg.gravity ? c->gy : nullptr;
+    A.src = c->src;
+    A.src_free = c->src_free;
+    A.phim = c->phim;
+    A.gxm = c->gxm;
+    A.gym = c->gym;
+    A.gxp = c->gxp;
+    A.gyp = c->gyp;
+    A.radx = nullptr;  // the radiation force reads the last P5's flux; P5 is off in reference mode
+    A.rady = nullptr;
+    A.push = c->push;
+    A.part = c->rpart;
+    A.part_best = c->rbest;
+    A.part_idx = c->ridx;
+    A.fin = c->rfin;
+    return A;
+}
+
 // P2 on the current state, then P9 (no floors) — what Twin::new does before step 0 (reference/mod.rs:129-177).
 static void initial_reductions(sr_ctx* c) {
     DtRecord rec{};
     SR_CUDA_TRY(cudaMemcpyAsync(c->rec, &rec, sizeof rec, cudaMemcpyHostToDevice, c->stream));
     SR_CUDA_TRY(cudaMemsetAsync(c->hreport, 0, 7 * sizeof(double), c->stream));
-    if (c->cfg.gravity) c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
     const sr_config& k = c->cfg;
+    if (ref_mode(c)) {
+        // reference/mod.rs:129-177: the hold's rule on the initial state, P2, then Δt_0
+        ref_hold_dt_launch(c->R, planes(c), c->held, nullptr, nullptr, 1, 0, c->part_rate, c->part_g, c->part_nf,
+                           k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec, c->stream);
+        if (k.gravity) c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
+        ref_hold_dt_launch(c->R, planes(c), c->held, k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 0, 1,
+                           c->part_rate, c->part_g, c->part_nf, k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec,
+                           c->stream);
+        SR_CUDA_TRY(cudaGetLastError());
+        return;
+    }
+    if (c->cfg.gravity) c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
     floors_dt_launch(c->H, planes(c), k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 0, c->part_rate,
                      c->part_g, c->part_nf, k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec, c->stream);
     SR_CUDA_TRY(cudaGetLastError());
@@ -223,6 +331,32 @@ static long long enqueue_step(sr_ctx* c, int cur, cudaStream_t s, cudaGraph_t ro
     dt_advance_launch(c->rec, s);
     if (k.gravity) c->grav.solve(U, c->phi, c->gx, c->gy, s);
     mark(1);
+    if (ref_mode(c)) {
+        // reference mode: P4 (step_held), P8's floors, the hold and P9 (reference/mod.rs:264-297; P5 is off)
+        if (k.hydro) {
+            RefArgs A = ref_args(c, cur);
+            if (k.gravity) {
+                ref_hydro_source_launch(A, s);
+                c->grav.solve(c->src, c->phim, c->gxm, c->gym, s);
+                c->grav.solve(c->src_free, c->phip, c->gxp, c->gyp, s);
+            }
+            mark(2);
+            ref_hydro_update_launch(A, k.gravity, s);
+            mark(3);
+            ref_hydro_finalize_launch(A, s);
+            U = c->U[1 - cur];
+        } else {
+            mark(2);
+            mark(3);
+        }
+        mark(4);
+        mark(5);
+        ref_floors_launch(c->R, U, s);
+        ref_hold_dt_launch(c->R, U, c->held, k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 1, 1,
+                           c->part_rate, c->part_g, c->part_nf, k.cfl, k.eta_g, k.dt_fixed, k.dt_cap, c->rec, s);
+        mark(6);
+        return heat_top;
+    }
     if (k.hydro) {
         HydroArgs A = hydro_args(c, cur);
         if (k.gravity) {
@@ -406,6 +540,14 @@ void sr_config_default(sr_config* c) {
     c->solve_tol = 1e-8;
     c->newton_heat = 1e-6;  // the reference GPU path's Newton stop (crates/sr-engine/shaders/heat.wgsl:355-357)
     c->newton_cell = 1e-3;
+    c->k1e = 21.3;  // assets/physics.json's cold pairs and hold; m_tov_sb of assets/calibration.json
+    c->k2e = 134.0;
+    c->k1n = 2.67;
+    c->k2n = 58.2;
+    c->sigma_hold = 10.0;
+    c->eta_hold = 0.1;
+    c->r_hold = 24.0;
+    c->m_tov = 4853.169981814195;
 }
 
 uint32_t sr_abi_version(void) { return SR_ABI_VERSION; }
@@ -426,8 +568,9 @@ sr_status sr_create(const sr_config* cfg, sr_ctx** out) {
         c->n = (size_t)c->w * c->h;
         const size_t n = c->n;
         SR_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
-        dalloc(&c->U[0], 4 * n);
-        dalloc(&c->U[1], 4 * n);
+        c->nc = (int)cfg->channels;
+        dalloc(&c->U[0], (size_t)c->nc * n);
+        dalloc(&c->U[1], (size_t)c->nc * n);
         dalloc(&c->phi, n);
         dalloc(&c->gx, n);
         dalloc(&c->gy, n);
@@ -448,6 +591,10 @@ sr_status sr_create(const sr_config* cfg, sr_ctx** out) {
         dalloc(&c->herr, 1);
         dalloc(&c->rec, 1);
         int fb = floors_dt_blocks(c->w, c->h);
+        if (c->nc == kRefChannels) {
+            fb = 148 * 8;  // the reference-mode Δt partials' grid at most
+            ref_setup(c);
+        }
         dalloc(&c->part_rate, (size_t)fb);
         dalloc(&c->part_g, (size_t)fb);
         dalloc(&c->part_nf, (size_t)fb);
@@ -471,8 +618,9 @@ void sr_destroy(sr_ctx* ctx) { ctx_free(ctx); }
 sr_status sr_upload(sr_ctx* c, const float* p, uint32_t nplanes) {
     return guarded(c, [&] {
         SR_REQUIRE(p, "sr_upload: null planes");
-        SR_REQUIRE(nplanes == 4, "sr_upload: this build carries 4 planes");
-        SR_CUDA_TRY(cudaMemcpyAsync(planes(c), p, sizeof(float) * 4 * c->n, cudaMemcpyHostToDevice, c->stream));
+        SR_REQUIRE((int)nplanes == c->nc, "sr_upload: the context carries " + std::to_string(c->nc) + " planes");
+        SR_CUDA_TRY(cudaMemcpyAsync(planes(c), p, sizeof(float) * c->nc * c->n, cudaMemcpyHostToDevice, c->stream));
+        if (c->held) SR_CUDA_TRY(cudaMemsetAsync(c->held, 0, c->n, c->stream));  // a new state: none held yet
         if (c->heat) heat_reset(c->heat, c->stream);
         initial_reductions(c);
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -483,9 +631,31 @@ sr_status sr_upload(sr_ctx* c, const float* p, uint32_t nplanes) {
 sr_status sr_readback(sr_ctx* c, float* p, uint32_t nplanes) {
     return guarded(c, [&] {
         SR_REQUIRE(p, "sr_readback: null planes");
-        SR_REQUIRE(nplanes == 4, "sr_readback: this build carries 4 planes");
-        SR_CUDA_TRY(cudaMemcpyAsync(p, planes(c), sizeof(float) * 4 * c->n, cudaMemcpyDeviceToHost, c->stream));
+        SR_REQUIRE((int)nplanes == c->nc, "sr_readback: the context carries " + std::to_string(c->nc) + " planes");
+        SR_CUDA_TRY(cudaMemcpyAsync(p, planes(c), sizeof(float) * c->nc * c->n, cudaMemcpyDeviceToHost, c->stream));
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+}
+
+sr_status sr_upload_held(sr_ctx* c, const uint32_t* mask) {
+    return guarded(c, [&] {
+        SR_REQUIRE(mask, "sr_upload_held: null mask");
+        SR_REQUIRE(c->held, "sr_upload_held: the hold is reference mode's (a context of 14 channels)");
+        std::vector<uint8_t> m(c->n);
+        for (size_t i = 0; i < c->n; i++) m[i] = mask[i] != 0;
+        SR_CUDA_TRY(cudaMemcpyAsync(c->held, m.data(), c->n, cudaMemcpyHostToDevice, c->stream));
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+}
+
+sr_status sr_read_held(sr_ctx* c, uint32_t* mask) {
+    return guarded(c, [&] {
+        SR_REQUIRE(mask, "sr_read_held: null mask");
+        SR_REQUIRE(c->held, "sr_read_held: the hold is reference mode's (a context of 14 channels)");
+        std::vector<uint8_t> m(c->n);
+        SR_CUDA_TRY(cudaMemcpyAsync(m.data(), c->held, c->n, cudaMemcpyDeviceToHost, c->stream));
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i < c->n; i++) mask[i] = m[i];
     });
 }
 

@@ -715,8 +715,9 @@ __global__ void floors_dt_kernel(HydroConst H, float* __restrict__ U, const floa
 // Δt_{n+1} = min(C / max rate, η_g / sqrt(max |g|)) (hydro.rs:618-634), the configured fixed Δt or cap, and the guard.
 // One CTA: each thread takes a strided share of the partials, then a shuffle and shared-memory tree (max and min are
 // exact in any order, so the result does not depend on the split).
-__global__ void dt_finalize_kernel(int nblocks, const float* part_rate, const float* part_g, const long long* part_nf,
-                                   double cfl, double eta_g, double dt_fixed, double dt_cap, DtRecord* rec) {
+__global__ void dt_finalize_kernel(int nblocks, int channels, const float* part_rate, const float* part_g,
+                                   const long long* part_nf, double cfl, double eta_g, double dt_fixed, double dt_cap,
+                                   DtRecord* rec) {
     float rate = 0.0f, gmax = 0.0f;
     long long nf = LLONG_MAX;
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
@@ -753,8 +754,8 @@ __global__ void dt_finalize_kernel(int nblocks, const float* part_rate, const fl
     rec->dt_next = dt;
     if (nf != LLONG_MAX && !rec->non_finite) {
         rec->non_finite = 1;
-        rec->nf_cell = nf / 4;
-        rec->nf_channel = (int)(nf % 4);
+        rec->nf_cell = nf / channels;
+        rec->nf_channel = (int)(nf % channels);
         rec->nf_step = rec->steps;
     }
 }
@@ -779,7 +780,14 @@ void floors_dt_launch(const HydroConst& H, float* U, const float* gx, const floa
     int nb = floors_dt_blocks(H.w, H.h);
     floors_dt_kernel<<<nb, 256, 0, s>>>(H, U, gx, gy, do_floors, part_rate, part_g, part_nf);
     sr_note_launch();
-    dt_finalize_kernel<<<1, 256, 0, s>>>(nb, part_rate, part_g, part_nf, cfl, eta_g, dt_fixed, dt_cap, rec);
+    dt_finalize_launch(nb, 4, part_rate, part_g, part_nf, cfl, eta_g, dt_fixed, dt_cap, rec, s);
+}
+
+void dt_finalize_launch(int nblocks, int channels, const float* part_rate, const float* part_g,
+                        const long long* part_nf, double cfl, double eta_g, double dt_fixed, double dt_cap,
+                        DtRecord* rec, cudaStream_t s) {
+    dt_finalize_kernel<<<1, 256, 0, s>>>(nblocks, channels, part_rate, part_g, part_nf, cfl, eta_g, dt_fixed, dt_cap,
+                                         rec);
     sr_note_launch();
 }
 

@@ -45,3 +45,7 @@ void floors_dt_launch(const HydroConst& H, float* U, const float* gx, const floa
                       float* part_g, long long* part_nf, double cfl, double eta_g, double dt_fixed, double dt_cap,
                       DtRecord* rec, cudaStream_t s);
 void dt_advance_launch(DtRecord* rec, cudaStream_t s);
+// Δt_{n+1} and the guard from per-CTA partials (the guard's codes are cell * channels + channel).
+void dt_finalize_launch(int nblocks, int channels, const float* part_rate, const float* part_g,
+                        const long long* part_nf, double cfl, double eta_g, double dt_fixed, double dt_cap,
+                        DtRecord* rec, cudaStream_t s);

@@ -9,9 +9,9 @@ most 16 objects of x, y, vx, vy, m) and ``resume`` (dt, dt_next, latch_since, bo
 and optionally rate, held, mass_carry) (parse_header, dump.rs:292-360). Every departure is refused with a message naming
 it, as Dump::from_bytes refuses (dump.rs:150-215).
 
-This build runs the 4-channel field update: ``Dump.state4()`` gives Σ, Σu, Σv, E for ``Step.upload``; the mass
-fractions, F, the rate and the mask are kept in the Dump for the caller (the reference-mode EOS that reads them is not
-part of this build).
+``load_into`` hands a dump to a Step: a reference-mode step (14 channels) takes every plane and the hold's mask; a
+4-channel step takes ``Dump.state4()`` (Σ, Σu, Σv, E). F and the rate are kept in the Dump for the caller (the
+reference-mode P5 that reads them is not part of this build).
 """
 from __future__ import annotations
 
@@ -233,8 +233,15 @@ def write(dump: Dump, path) -> None:
 
 
 def load_into(step, dump: Dump) -> None:
-    """Uploads the dump's 4 field channels into `step` (a sandbox_reactions_b200.engine.Step of the same world)."""
+    """Uploads the dump into `step` (a sandbox_reactions_b200.engine.Step of the same world): a 4-channel step takes
+    Σ, Σu, Σv, E; a reference-mode step (14 channels) takes every plane and, when the dump holds one, the hold's mask
+    (the reference's resume: State::upload, then State::upload_held, state.rs:198-279)."""
     c, h, w = step.shape
     if (h, w) != (dump.height, dump.width):
         raise DumpError(f"dump world {dump.width} x {dump.height}, the step's {w} x {h}")
+    if c == len(CHANNELS):
+        step.upload(np.ascontiguousarray(dump.planes, np.float32))
+        if dump.held is not None:
+            step.upload_held(dump.held)
+        return
     step.upload(dump.state4())

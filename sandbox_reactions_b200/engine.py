@@ -49,6 +49,8 @@ def load_library(path: str = LIB_PATH):
     L.sr_upload.argtypes = [P, F, C.c_uint32]
     L.sr_readback.argtypes = [P, F, C.c_uint32]
     L.sr_upload_opacity.argtypes = [P, F]
+    L.sr_upload_held.argtypes = [P, C.POINTER(C.c_uint32)]
+    L.sr_read_held.argtypes = [P, C.POINTER(C.c_uint32)]
     L.sr_step.argtypes = [P, C.c_uint32]
     L.sr_read_dt.argtypes = [P, C.POINTER(sr_dt_report)]
     L.sr_read_heat.argtypes = [P, C.POINTER(sr_heat_report)]
@@ -91,7 +93,8 @@ def load_library(path: str = LIB_PATH):
         getattr(L, name).restype = C.c_int
     L.sr_last_error.restype = C.c_char_p
     L.sr_last_error.argtypes = [P]
-    for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_step", "sr_read_dt",
+    for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_upload_held", "sr_read_held",
+                 "sr_step", "sr_read_dt",
                  "sr_read_heat", "sr_gravity_field", "sr_heat_flux", "sr_set_edge_mode", "sr_set_heat_precond",
                  "sr_set_heat_limits", "sr_set_timing", "sr_read_cost", "sr_heat_first_solve"):
         getattr(L, name).restype = C.c_int
@@ -146,14 +149,14 @@ class Step:
 
     @property
     def shape(self):
-        return (4, self.config.height, self.config.width)
+        return (self.config.channels, self.config.height, self.config.width)
 
     # ---- State::upload / readback (state.rs:251-279)
     def upload(self, planes: np.ndarray):
         p = np.ascontiguousarray(planes, dtype=np.float32)
         if p.shape != self.shape:
             raise SrError(1, f"planes of shape {p.shape}, expected {self.shape}")
-        self._check(self.lib.sr_upload(self._h, _fptr(p), 4))
+        self._check(self.lib.sr_upload(self._h, _fptr(p), self.shape[0]))
 
     def upload_opacity(self, kappa: np.ndarray):
         k = np.ascontiguousarray(kappa, dtype=np.float32)
@@ -164,8 +167,20 @@ class Step:
     def readback(self, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
             out = np.empty(self.shape, dtype=np.float32)
-        self._check(self.lib.sr_readback(self._h, _fptr(out), 4))
+        self._check(self.lib.sr_readback(self._h, _fptr(out), self.shape[0]))
         return out
+
+    # ---- State::upload_held / read_held (state.rs:198-250), reference mode
+    def upload_held(self, mask: np.ndarray):
+        m = np.ascontiguousarray(mask, dtype=np.uint32)
+        if m.shape != self.shape[1:]:
+            raise SrError(1, f"mask of shape {m.shape}, expected {self.shape[1:]}")
+        self._check(self.lib.sr_upload_held(self._h, m.ctypes.data_as(C.POINTER(C.c_uint32))))
+
+    def read_held(self) -> np.ndarray:
+        m = np.zeros(self.shape[1:], np.uint32)
+        self._check(self.lib.sr_read_held(self._h, m.ctypes.data_as(C.POINTER(C.c_uint32))))
+        return m
 
     # ---- Step::run (step/mod.rs:703-718)
     def run(self, steps: int = 1):

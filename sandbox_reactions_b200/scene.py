@@ -670,6 +670,27 @@ class Scene:
                       pin_temperature=self.test.pin_temperature, flux_limiter=self.test.flux_limiter,
                       opacity_plane=sw.heat)
 
+    def ref_config(self, world=None, strict: bool = True, m_tov: float = 4853.169981814195) -> Config:
+        """The scene as a reference-mode Config (14 channels: the reference's EOS with the cold pairs of its physics,
+        the species, the hold), for the planes ``Scene.planes`` lays down. ``m_tov`` is m_tov_sb, the hold's gate
+        (assets/calibration.json's value for the shipped physics). With `strict`, refuses by name the switches the
+        reference-mode field update does not run (heat, reactions, neutrinos, sinks); without it they are left out."""
+        w, h = self._world(world)
+        v = self.physics().values
+        sw = self.switches
+        if strict:
+            for name in ("heat", "reactions", "neutrinos", "sinks"):
+                if getattr(sw, name):
+                    raise SceneError(f"switches.{name}: on, but the reference-mode field update runs hydro and "
+                                     f"gravity only: switch it off in the scene or load with strict=False")
+        return Config(width=w, height=h, channels=N_CHANNELS, edge=self.edge, gravity=sw.gravity, hydro=sw.hydro,
+                      heat=False, kernel="self_cell", limiter="mc", thermal_bracket=True, gamma=2.0, mu=1.0,
+                      t_floor=v["t_floor"], sigma_vac=v["sigma_vac"], sigma_floor=v["sigma_floor"], cfl=v["cfl"],
+                      eta_g=v["eta_g"], G=1.0, a_r=v["a_r"], c_sb=v["c_sb"], kappa0=v["kappa0"],
+                      k_cond=v["k_cond"], k1e=v["k1e"], k2e=v["k2e"], k1n=v["k1n"], k2n=v["k2n"],
+                      kappa_dust=v["kappa_dust"], t_dust=v["t_dust"], sigma_hold=v["sigma_hold"],
+                      eta_hold=v["eta_hold"], r_hold=v["r_hold"], m_tov=m_tov)
+
     def _heat_mu(self, w, h, physics, planes):
         """The gas cells' mu (Sigma >= sigma_vac), which must be one: from the compositions of the objects that
         cover gas cells, and hydrogen where the floor state is gas."""

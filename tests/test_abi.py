@@ -40,7 +40,7 @@ def test_the_config_defaults_match_the_library():
         if name.startswith("reserved") or name in ("width", "height"):
             continue
         assert getattr(c, name) == getattr(py, name), name
-    assert lib.sr_abi_version() == 2
+    assert lib.sr_abi_version() == 3
 
 
 def test_create_refuses_a_bad_world_without_touching_a_device():

@@ -1,0 +1,178 @@
+"""Reference mode on the GPU (14 channels: the reference's EOS with species and cold pressures, held cells) through the
+C ABI against the oracle's reference-mode twin (oracle/sr_oracle_ref.c; reference/mod.rs:129-297 without P5):
+
+  - scenes/thin_cell.bin (tests/golden/thin_cell.npz): one step of P4 alone, leave edges, the hold's rule on the cut —
+    Σ and E within rel L1 1e-5 of the twin, the momentum within 3e-5, each species' fraction within 1e-5
+    mass-weighted (the measures `compare` states), the same held cells, and no free gas cell faster than 10x its free
+    neighbours' largest (crates/sr-engine/tests/gpu/sod.rs:689-704);
+  - a two-species shock tube (hydrogen | helium, the reference's scenes/ref_sod.json laid down at 128 x 64 with the cold
+    pairs off, bounce edges): 1 and 40 steps, the species advected;
+  - a cold disk under the shipped physics (the cold pairs on, gravity, leave edges): 3 steps;
+  - a dense cold core the hold's rule holds, with gravity: 4 steps — the held cells behind their reflecting walls, the
+    pull on them from the free cells' field, the sticky wall; the mask equal to the twin's after every step;
+  - the hold's mask through sr_upload_held / sr_read_held."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from sandbox_reactions_b200.abi import Config
+from sandbox_reactions_b200.engine import Step
+from sandbox_reactions_b200.scene import Scene
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def rel_l1(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    d = np.abs(b).sum()
+    return np.abs(a - b).sum() / d if d > 0 else np.abs(a).sum()
+
+
+def compare(gpu, ref, bar, what):
+    """Σ and E by rel L1 <= bar; the two momentum planes together, Σ|ΔΣu| + |ΔΣv| over Σ|Σu| + |Σv| (a tube along x
+    holds Σv = 0), within 3x bar: where the cold pressure dominates, one step moves the momentum by more than it holds,
+    and a 1e-7 change of the f32 input alone moves the twin's Σu by 6e-6 in rel L1 (the cold disk below); each species
+    by its mass-weighted error in the fraction, Σ_cells Σ|ΔX| / Σ_cells Σ, within bar — a trace species (X ~ 1e-20
+    beside X ~ 1) is the small difference of large fluxes, and the same 1e-7 change moves its own rel L1 by ~1e-4
+    (scenes/thin_cell.bin), so its error is measured against the gas's mass, as its mass moves."""
+    g = [np.asarray(gpu[k], np.float64) for k in range(14)]
+    errs = {"sigma": rel_l1(g[0], ref[0]), "E": rel_l1(g[3], ref[3]),
+            "momentum": (np.abs(g[1] - ref[1]).sum() + np.abs(g[2] - ref[2]).sum()) /
+                        max(np.abs(ref[1]).sum() + np.abs(ref[2]).sum(), 1e-300) / 3.0}
+    sig = np.asarray(ref[0], np.float64)
+    for s in range(10):
+        errs[f"X{s}"] = float((sig * np.abs(g[4 + s] - ref[4 + s])).sum() / sig.sum())
+    worst = max(errs.values())
+    assert worst <= bar, (what, {k: f"{v:.2e}" for k, v in errs.items()})
+    return worst
+
+
+def run_both(cfg, P, steps, mask=None):
+    with Step(cfg) as s:
+        s.upload(P)
+        if mask is not None:
+            s.upload_held(mask)
+        masks = [s.read_held()]
+        outs = []
+        for _ in range(steps):
+            s.run(1)
+            outs.append(s.readback())
+            masks.append(s.read_held())
+        clock = s.read_dt()
+    twin = O.RefTwin(cfg, P.astype(np.float64), mask)
+    tm = [twin.state()[1]]
+    touts = []
+    for _ in range(steps):
+        twin.step()
+        st, m = twin.state()
+        touts.append(st)
+        tm.append(m)
+    return outs, masks, clock, touts, tm, twin
+
+
+def test_the_thin_cell_steps_like_the_twin_and_takes_no_leap():
+    f = np.load(os.path.join(HERE, "golden", "thin_cell.npz"))
+    P = f["planes"]
+    cfg = Config(width=64, height=64, channels=14, edge="leave", gravity=False, hydro=True)
+    outs, masks, _, touts, tm, _ = run_both(cfg, P, 1)
+    compare(outs[0], touts[0], 1e-5, "thin cell")
+    assert np.array_equal(masks[0] != 0, tm[0] != 0) and np.array_equal(masks[1] != 0, tm[1] != 0)
+    from test_oracle_ref import worst_leap
+    ratio, _, _ = worst_leap(outs[0].astype(np.float64), masks[1])
+    assert ratio <= 10.0, ratio
+
+
+REF_SOD = """{"version": 1,
+ "world": {"width": 128, "height": 64, "edge": "bounce"},
+ "slowdown": false,
+ "switches": {"gravity": false, "heat": false, "reactions": false, "neutrinos": false, "sinks": false},
+ "objects": [
+   {"kind": "rect", "x0": 0, "y0": 0, "w": 64, "h": 64, "sigma": 1.0, "pressure": 1.0, "composition": {"H": 1.0},
+    "v": [0, 0]},
+   {"kind": "rect", "x0": 64, "y0": 0, "w": 64, "h": 64, "sigma": 0.125, "pressure": 0.1,
+    "composition": {"He": 1.0}, "v": [0, 0]}
+ ],
+ "overrides": {"k1e": 0, "k2e": 0, "k1n": 0, "k2n": 0}}"""
+
+
+def test_a_two_species_tube_advects_its_species_like_the_twin():
+    sc = Scene.parse(REF_SOD)
+    P, _ = sc.planes()
+    cfg = sc.ref_config()
+    outs, _, clock, touts, _, twin = run_both(cfg, P, 40)
+    compare(outs[0], touts[0], 1e-5, "one step")
+    compare(outs[-1], touts[-1], 1e-4, "40 steps")
+    assert abs(clock.sim_time - twin.clock()["sim_time"]) <= 1e-5 * twin.clock()["sim_time"]
+    # mass of each species conserved by the walls (bounce)
+    for s in range(10):
+        m0 = (P[0].astype(np.float64) * P[4 + s]).sum()
+        m1 = (outs[-1][0].astype(np.float64) * outs[-1][4 + s]).sum()
+        assert abs(m1 - m0) <= 1e-5 * max(m0, 1e-30) + 1e-9
+
+
+COLD_DISK = """{"version": 1,
+ "world": {"width": 96, "height": 96, "edge": "leave"},
+ "slowdown": false,
+ "switches": {"gravity": true, "hydro": true, "heat": false, "reactions": false, "neutrinos": false, "sinks": false},
+ "objects": [
+   {"kind": "disk", "x": 48, "y": 48, "a": 30, "sigma_c": 2.0, "t": 0.5,
+    "composition": {"H": 0.7, "He": 0.28, "C": 0.01, "O": 0.01}, "v": [0.1, -0.05]}
+ ]}"""
+
+
+def test_a_disk_under_the_shipped_cold_pressures_steps_like_the_twin():
+    sc = Scene.parse(COLD_DISK)
+    P, _ = sc.planes()
+    cfg = sc.ref_config()
+    assert cfg.k1e > 0 and cfg.k1n > 0
+    outs, _, _, touts, _, _ = run_both(cfg, P, 3)
+    compare(outs[0], touts[0], 1e-5, "one step")
+    compare(outs[-1], touts[-1], 2e-5, "three steps")
+
+
+def held_core_world():
+    """A 96² leave-edge world: thin warm hydrogen, a rotating disk of denser gas and, at its centre, a core dense and
+    cold enough that the hold's rule takes it (Σ 24 >= σ_hold, ε_th = 0.05 ε_cold <= η_hold ε_cold)."""
+    n = 96
+    cfg = Config(width=n, height=n, channels=14, edge="leave", gravity=True, hydro=True)
+    yy, xx = np.mgrid[0:n, 0:n] + 0.5
+    r = np.hypot(xx - 48, yy - 48)
+    s = np.where(r < 30, 2.0 * np.sqrt(np.clip(1 - (r / 30) ** 2, 0, 1)) + 0.01, 0.01)
+    core = r < 3.5
+    s = np.where(core, 24.0, s)
+    vx, vy = -(yy - 48) * 0.02, (xx - 48) * 0.02
+    P = np.zeros((14, n, n))
+    P[0] = s
+    P[1], P[2] = s * vx, s * vy
+    P[4] = 0.75
+    P[5] = 0.25
+    inv_mu, ye, _ = O.composition([0.75, 0.25] + [0.0] * 8)
+    ln_e = O.cold_table(cfg.k1e, cfg.k2e)
+    cold = np.array([O.cold_table_u(ln_e, ye * v) / v for v in s.ravel()]).reshape(s.shape)
+    eps = np.where(core, 0.05 * cold, 0.3 * inv_mu * 10)
+    P[3] = s * (eps + cold) + 0.5 * s * (vx * vx + vy * vy)
+    return cfg, P.astype(np.float32)
+
+
+def test_a_held_core_behind_its_walls_steps_like_the_twin():
+    cfg, P = held_core_world()
+    outs, masks, _, touts, tm, _ = run_both(cfg, P, 4)
+    assert (tm[0] != 0).sum() > 0, "the rule holds the core"
+    for k in range(5):
+        assert np.array_equal(masks[k] != 0, tm[k] != 0), k
+    for k in range(4):
+        compare(outs[k], touts[k], 2e-5, f"step {k + 1}")
+
+
+def test_the_hold_mask_round_trips():
+    cfg, P = held_core_world()
+    with Step(cfg.replace(gravity=False)) as s:
+        s.upload(P)
+        rng = np.random.default_rng(3)
+        m = (rng.random((cfg.height, cfg.width)) < 0.1).astype(np.uint32)
+        s.upload_held(m)
+        assert np.array_equal(s.read_held(), m)
