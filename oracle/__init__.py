@@ -110,6 +110,10 @@ def lib():
         L.or_ref_twin_state.argtypes = [C.c_void_p, _D, U8]
         L.or_ref_twin_clock.argtypes = [C.c_void_p, _D]
         L.or_ref_twin_books.argtypes = [C.c_void_p, _D]
+        L.or_ref_twin_heat.argtypes = [C.c_void_p, C.POINTER(or_heat_report), _D, _D]
+        L.or_ref_heat_sides.argtypes = [P, _D, C.c_int64, C.c_int64, _D, _D, _D]
+        L.or_ref_heat_step.argtypes = [P, _D, C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double, C.c_double,
+                                       C.POINTER(or_heat_report), _D, _D]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_get_threads.restype = C.c_int
         _lib = L
@@ -480,3 +484,31 @@ class RefTwin:
         out = np.zeros(4)
         lib().or_ref_twin_books(self._t, _p(out))
         return {"held": (out[0], out[1]), "vacuum_reset": out[2], "floor_added": out[3]}
+
+    def heat(self):
+        h, w = self.cfg.height, self.cfg.width
+        rep = or_heat_report()
+        fx, fy = np.zeros((h, w + 1)), np.zeros((h + 1, w))
+        lib().or_ref_twin_heat(self._t, C.byref(rep), _p(fx), _p(fy))
+        return rep, fx, fy
+
+
+def ref_heat_sides(cfg: Config, planes: np.ndarray):
+    """P5's sides of a (14, H, W) state: T⁰, κ and 1/μ per cell (heat.rs:215-231)."""
+    p = _f64(planes)
+    _, h, w = p.shape
+    t0, kappa, inv_mu = np.zeros((h, w)), np.zeros((h, w)), np.zeros((h, w))
+    c = cfg.to_c()
+    lib().or_ref_heat_sides(C.byref(c), _p(p), w, h, _p(t0), _p(kappa), _p(inv_mu))
+    return t0, kappa, inv_mu
+
+
+def ref_heat_step(cfg: Config, planes: np.ndarray, dt: float, tol=1e-12, newton_heat=1e-12, newton_cell=1e-10):
+    """One reference-mode implicit FLD step on (14, H, W) planes; returns (planes, report, fx, fy)."""
+    p = _f64(planes).copy()
+    _, h, w = p.shape
+    fx, fy = np.zeros((h, w + 1)), np.zeros((h + 1, w))
+    rep = or_heat_report()
+    c = cfg.to_c()
+    lib().or_ref_heat_step(C.byref(c), _p(p), w, h, dt, tol, newton_heat, newton_cell, C.byref(rep), _p(fx), _p(fy))
+    return p, rep, fx, fy

@@ -759,10 +759,16 @@ void or_floors(const sr_config* cfg, double* planes, int64_t w, int64_t h) {
 
 double or_lambda(double r) { return (2.0 + r) / (6.0 + 3.0 * r + r * r); } /* heat.rs:132-134 */
 
-typedef struct { int gas; double t, s, kappa, inv_c; } side; /* heat.rs:136-154; inv_c: 1/(μ(γ-1)) */
+typedef struct { int gas; double t, s, kappa, inv_c; } side; /* heat.rs:136-154; C = Σ inv_c, inv_c = 1/(μ(γ-1)) */
+
+/* Reference mode's sides, per cell: T⁰ (T_floor off the gas), κ and 1/μ from the cell's species (heat.rs:215-226) */
+typedef struct {
+    const double *t, *kappa, *inv_mu;
+} ref_sides;
 
 typedef struct {
     const sr_config* cfg;
+    const ref_sides* rs;
     double gm1, mu, t_floor, sigma_vac, sigma_floor, a_r, c_sb, k_cond, chi;
     int limiter_on;
     int64_t w, h;
@@ -770,14 +776,24 @@ typedef struct {
     double *c, *kx, *ky, vac;
 } net;
 
-static double cap_of(const net* N, const side* s) { return s->s / (N->mu * N->gm1); } /* C = Σ/(μ(γ-1)) */
+/* C = Σ/(μ(γ-1)); reference mode: Σ/μ of the side's own species */
+static double cap_of(const net* N, const side* s) { return N->rs ? s->s * s->inv_c : s->s / (N->mu * N->gm1); }
 
 static side side_of(const net* N, const double* planes, const double* kappa, int64_t i) {
     /* heat.rs:215-226: the floor state below Σ_vac, else T from the thermal energy (floored) */
     int64_t n = N->w * N->h;
     double s = planes[i];
-    double k = kappa ? kappa[i] : N->cfg->kappa0;
     side o;
+    if (N->rs) {
+        o.gas = s >= N->sigma_vac;
+        o.t = N->rs->t[i];
+        o.s = o.gas ? s : N->sigma_floor;
+        o.kappa = N->rs->kappa[i];
+        o.inv_c = N->rs->inv_mu[i];
+        return o;
+    }
+    double k = kappa ? kappa[i] : N->cfg->kappa0;
+    o.inv_c = 1.0 / (N->mu * N->gm1);
     if (s < N->sigma_vac) {
         o.gas = 0;
         o.t = N->t_floor;
@@ -797,8 +813,8 @@ static side side_of(const net* N, const double* planes, const double* kappa, int
     return o;
 }
 
-static side vacuum_beyond(const net* N, const side* g) { /* heat.rs:234-237 */
-    side o = {0, N->t_floor, N->sigma_floor, g->kappa, 0.0};
+static side vacuum_beyond(const net* N, const side* g) { /* heat.rs:234-237: the gas side's κ and μ */
+    side o = {0, N->t_floor, N->sigma_floor, g->kappa, g->inv_c};
     return o;
 }
 
@@ -843,8 +859,9 @@ static double face_coef(const net* N, const side* a, const side* b) {
 }
 
 static void net_build(net* N, const sr_config* cfg, const double* planes, const double* kappa, int64_t w, int64_t h,
-                      side** sides_out) {
+                      side** sides_out, const ref_sides* rs) {
     N->cfg = cfg;
+    N->rs = rs;
     N->gm1 = cfg->gamma - 1.0;
     N->mu = cfg->mu;
     N->t_floor = cfg->t_floor;
@@ -1070,13 +1087,30 @@ static void commit_limited(const net* N, double* planes, const double* u, const 
     free(fx); free(fy); free(scale);
 }
 
+static void heat_step_impl(const sr_config* cfg, double* planes, const double* kappa, const ref_sides* rs, int64_t w,
+                           int64_t h, double dt, double tol, double newton_heat, double newton_cell, or_heat_report* rep,
+                           double* fxo, double* fyo);
+
 void or_heat_step(const sr_config* cfg, double* planes, const double* kappa, int64_t w, int64_t h, double dt,
                   double tol, double newton_heat, double newton_cell, or_heat_report* rep, double* fxo, double* fyo) {
+    heat_step_impl(cfg, planes, kappa, NULL, w, h, dt, tol, newton_heat, newton_cell, rep, fxo, fyo);
+}
+
+void or_heat_step_sides(const sr_config* cfg, double* planes, int64_t w, int64_t h, double dt, double tol,
+                        double newton_heat, double newton_cell, const double* t0, const double* kappa,
+                        const double* inv_mu, or_heat_report* rep, double* fxo, double* fyo) {
+    ref_sides rs = {t0, kappa, inv_mu};
+    heat_step_impl(cfg, planes, NULL, &rs, w, h, dt, tol, newton_heat, newton_cell, rep, fxo, fyo);
+}
+
+static void heat_step_impl(const sr_config* cfg, double* planes, const double* kappa, const ref_sides* rs, int64_t w,
+                           int64_t h, double dt, double tol, double newton_heat, double newton_cell, or_heat_report* rep,
+                           double* fxo, double* fyo) {
     /* heat.rs:453-536 */
     int64_t n = w * h;
     net N;
     side* sides;
-    net_build(&N, cfg, planes, kappa, w, h, &sides);
+    net_build(&N, cfg, planes, kappa, w, h, &sides, rs);
     double* t0 = (double*)malloc(sizeof(double) * (size_t)n);
     double* u0 = (double*)malloc(sizeof(double) * (size_t)n);
     int64_t ngas = 0;
@@ -1195,7 +1229,7 @@ void or_heat_law(const sr_config* cfg, const double* planes, const double* kappa
     /* heat.rs:303-309 */
     net N;
     side* sides;
-    net_build(&N, cfg, planes, kappa, w, h, &sides);
+    net_build(&N, cfg, planes, kappa, w, h, &sides, NULL);
     int64_t n = w * h;
     double* u = (double*)malloc(sizeof(double) * (size_t)n);
     for (int64_t i = 0; i < n; i++) u[i] = u_of(&N, sides[i].t);
@@ -1210,7 +1244,7 @@ void or_heat_system(const sr_config* cfg, const double* planes, const double* ka
     /* heat.rs:476-489 at the first iterate (t = T⁰, u = u⁰) */
     net N;
     side* sides;
-    net_build(&N, cfg, planes, kappa, w, h, &sides);
+    net_build(&N, cfg, planes, kappa, w, h, &sides, NULL);
     int64_t n = w * h;
     for (int64_t i = 0; i < n; i++) {
         gas[i] = N.gas[i];

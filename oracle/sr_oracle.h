@@ -70,6 +70,10 @@ double or_lambda(double r);
  * (heat.rs SOLVE_TOL = 1e-12), `newton_heat`/`newton_cell` the pass rules (1e-12 / 1e-10 in the twin). */
 void or_heat_step(const sr_config* cfg, double* planes, const double* kappa, int64_t w, int64_t h, double dt,
                   double tol, double newton_heat, double newton_cell, or_heat_report* rep, double* fx, double* fy);
+/* The same step on per-cell sides (reference mode): T⁰, κ and 1/μ of every cell (T_floor off the gas); C = Σ/μ. */
+void or_heat_step_sides(const sr_config* cfg, double* planes, int64_t w, int64_t h, double dt, double tol,
+                        double newton_heat, double newton_cell, const double* t0, const double* kappa,
+                        const double* inv_mu, or_heat_report* rep, double* fxo, double* fyo);
 /* The frozen law's flux on the start state (heat.rs:303-309). */
 void or_heat_law(const sr_config* cfg, const double* planes, const double* kappa, int64_t w, int64_t h, double* fx,
                  double* fy);
@@ -149,6 +153,13 @@ void or_ref_twin_state(const or_ref_twin* t, double* planes, uint8_t* mask);
 void or_ref_twin_clock(const or_ref_twin* t, double* out4);
 /* [held x, held y, vacuum_reset, floor_added] booked since the twin was made */
 void or_ref_twin_books(const or_ref_twin* t, double* out4);
+/* The last P5's report and face fluxes. */
+void or_ref_twin_heat(const or_ref_twin* t, or_heat_report* rep, double* fx, double* fy);
+/* P5's sides of a 14-channel state (heat.rs:215-231) and one reference-mode implicit step on them. */
+void or_ref_heat_sides(const sr_config* cfg, const double* planes, int64_t w, int64_t h, double* t0, double* kappa,
+                       double* inv_mu);
+void or_ref_heat_step(const sr_config* cfg, double* planes, int64_t w, int64_t h, double dt, double tol,
+                      double newton_heat, double newton_cell, or_heat_report* rep, double* fx, double* fy);
 
 #ifdef __cplusplus
 }

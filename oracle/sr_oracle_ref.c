@@ -959,6 +959,46 @@ void or_ref_hold(const sr_config* cfg, double* planes, int64_t w, int64_t h, uin
     }
 }
 
+/* ======================================================================= P5 (reference/heat.rs) */
+
+void or_ref_heat_sides(const sr_config* cfg, const double* planes, int64_t w, int64_t h, double* t0, double* kappa,
+                       double* inv_mu) {
+    /* heat.rs:215-231: each cell's T⁰ (T_floor below Σ_vac), κ = κ₀(1 + X_H) plus κ_dust Z_met below T_dust, 1/μ */
+    eos_t E;
+    eos_init(&E, cfg);
+    const int64_t n = w * h;
+    for (int64_t i = 0; i < n; i++) {
+        double x[NS];
+        for (int k = 0; k < NS; k++) x[k] = planes[(4 + k) * n + i];
+        comp_t c = composition(x);
+        double mu = 1.0 / c.inv_mu, s = planes[i], t;
+        if (s < cfg->sigma_vac) {
+            t = E.t_floor;
+        } else {
+            double eps = eos_thermal(&E, planes[3 * n + i], s, planes[n + i], planes[2 * n + i], c.y_e, x[ID_N], mu,
+                                     NULL);
+            t = mu * eps;
+        }
+        t0[i] = t;
+        kappa[i] = cfg->kappa0 * (1.0 + x[ID_H]) + (t < cfg->t_dust ? cfg->kappa_dust * c.z_met : 0.0);
+        inv_mu[i] = c.inv_mu;
+    }
+}
+
+void or_ref_heat_step(const sr_config* cfg, double* planes, int64_t w, int64_t h, double dt, double tol,
+                      double newton_heat, double newton_cell, or_heat_report* rep, double* fx, double* fy) {
+    /* heat.rs:453-592 on the reference's own sides: C = Σ/μ, T from the EOS with the cold energy, κ of the species */
+    const int64_t n = w * h;
+    double* t0 = (double*)malloc(sizeof(double) * (size_t)n);
+    double* kappa = (double*)malloc(sizeof(double) * (size_t)n);
+    double* inv_mu = (double*)malloc(sizeof(double) * (size_t)n);
+    or_ref_heat_sides(cfg, planes, w, h, t0, kappa, inv_mu);
+    or_heat_step_sides(cfg, planes, w, h, dt, tol, newton_heat, newton_cell, t0, kappa, inv_mu, rep, fx, fy);
+    free(t0);
+    free(kappa);
+    free(inv_mu);
+}
+
 /* ======================================================================= the twin (reference/mod.rs) */
 
 struct or_ref_twin {
@@ -972,6 +1012,8 @@ struct or_ref_twin {
     double held[2], booked[2];
     double dt, dt_next, sim_time;
     int64_t steps;
+    or_heat_report heat;  /* the last P5's report */
+    double *hfx, *hfy;    /* the last P5's face fluxes */
 };
 
 static void ref_twin_gravity(or_ref_twin* t) {
@@ -1021,6 +1063,8 @@ void or_ref_twin_free(or_ref_twin* t) {
     free(t->gy);
     free(t->radx);
     free(t->rady);
+    free(t->hfx);
+    free(t->hfy);
     free(t);
 }
 
@@ -1036,7 +1080,8 @@ void or_ref_twin_set_flux(or_ref_twin* t, const double* fx, const double* fy) {
 }
 
 void or_ref_twin_step(or_ref_twin* t) {
-    /* mod.rs:264-297: P1, P2, P4 (step_held), P8 (floors, then the hold), P9 */
+    /* mod.rs:264-297: P1, P2, P4 (step_held), P5 (its F the next step's radiation force), P8 (floors, then the hold),
+     * P9 */
     double dt = t->dt_next;
     t->dt = dt;
     t->sim_time += dt;
@@ -1047,6 +1092,23 @@ void or_ref_twin_step(or_ref_twin* t) {
                           t->cfg.gravity ? t->gy : NULL, t->mask, t->radx, t->rady, &rep);
         t->held[0] += rep.spared[0];
         t->held[1] += rep.spared[1];
+    }
+    if (t->cfg.heat) {
+        const int64_t w = t->w, h = t->h, n = w * h;
+        if (!t->hfx) {
+            t->hfx = (double*)malloc(sizeof(double) * (size_t)((w + 1) * h));
+            t->hfy = (double*)malloc(sizeof(double) * (size_t)(w * (h + 1)));
+            t->radx = (double*)malloc(sizeof(double) * (size_t)n);
+            t->rady = (double*)malloc(sizeof(double) * (size_t)n);
+        }
+        /* the twin's tolerances (heat.rs:59-62) */
+        or_ref_heat_step(&t->cfg, t->planes, w, h, dt, 1e-12, 1e-12, 1e-10, &t->heat, t->hfx, t->hfy);
+        /* heat.rs:100-112: the cell-centred F, the mean of a cell's two faces on each axis */
+        for (int64_t y = 0; y < h; y++)
+            for (int64_t x = 0; x < w; x++) {
+                t->radx[y * w + x] = 0.5 * (t->hfx[y * (w + 1) + x] + t->hfx[y * (w + 1) + x + 1]);
+                t->rady[y * w + x] = 0.5 * (t->hfy[y * w + x] + t->hfy[(y + 1) * w + x]);
+            }
     }
     double booked[2];
     or_ref_floors(&t->cfg, t->planes, t->w, t->h, booked);
@@ -1068,6 +1130,13 @@ void or_ref_twin_clock(const or_ref_twin* t, double* out4) {
     out4[1] = t->dt_next;
     out4[2] = t->sim_time;
     out4[3] = (double)t->steps;
+}
+
+void or_ref_twin_heat(const or_ref_twin* t, or_heat_report* rep, double* fx, double* fy) {
+    if (rep) *rep = t->heat;
+    const int64_t w = t->w, h = t->h;
+    if (fx && t->hfx) memcpy(fx, t->hfx, sizeof(double) * (size_t)((w + 1) * h));
+    if (fy && t->hfy) memcpy(fy, t->hfy, sizeof(double) * (size_t)(w * (h + 1)));
 }
 
 void or_ref_twin_books(const or_ref_twin* t, double* out4) {

@@ -50,6 +50,7 @@ struct sr_ctx {
     uint8_t* held = nullptr;      // the hold's mask
     float *src_free = nullptr, *phip = nullptr, *gxp = nullptr, *gyp = nullptr;  // the pull on the held cells
     float* push = nullptr;        // each cell's radiation push
+    float *radx = nullptr, *rady = nullptr;  // the last P5's cell-centred flux, the next P4's radiation force
     double* rpart = nullptr;      // the reference-mode P4's per-CTA partials and their reduction
     float* rbest = nullptr;
     int* ridx = nullptr;
@@ -87,7 +88,7 @@ static void validate(const sr_config& c) {
     SR_REQUIRE(c.channels == 4 || c.channels == kRefChannels,
                "channels must be 4 (Σ, Σu, Σv, E) or 14 (reference mode: the ten mass fractions after them)");
     if (c.channels == kRefChannels) {
-        SR_REQUIRE(!c.heat, "reference mode (14 channels) steps P4, P2, P8 and P9; its P5 is not built: heat must be off");
+        SR_REQUIRE(!c.opacity_plane, "reference mode (14 channels) takes κ from each cell's species: no opacity plane");
         SR_REQUIRE(c.k1e >= 0.0 && c.k2e >= 0.0 && c.k1n >= 0.0 && c.k2n >= 0.0, "the cold pairs' K must be >= 0");
         SR_REQUIRE((c.k1e > 0.0) == (c.k2e > 0.0) && (c.k1n > 0.0) == (c.k2n > 0.0),
                    "a cold pair is on or off as a whole (k1e/k2e, k1n/k2n)");
@@ -147,7 +148,7 @@ static void ctx_free(sr_ctx* c) {
     cudaFree(c->src); cudaFree(c->phim); cudaFree(c->gxm); cudaFree(c->gym);
     cudaFree(c->kappa);
     cudaFree(c->table); cudaFree(c->held); cudaFree(c->src_free); cudaFree(c->phip); cudaFree(c->gxp);
-    cudaFree(c->gyp); cudaFree(c->push); cudaFree(c->rpart); cudaFree(c->rbest); cudaFree(c->ridx); cudaFree(c->rfin);
+    cudaFree(c->gyp); cudaFree(c->push); cudaFree(c->radx); cudaFree(c->rady); cudaFree(c->rpart); cudaFree(c->rbest); cudaFree(c->ridx); cudaFree(c->rfin);
     if (c->grav_ready) c->grav.destroy();
     cudaFree(c->part_d); cudaFree(c->part_best); cudaFree(c->part_idx); cudaFree(c->hreport); cudaFree(c->herr);
     cudaFree(c->rec); cudaFree(c->part_rate); cudaFree(c->part_g); cudaFree(c->part_nf);
@@ -227,6 +228,10 @@ static void ref_setup(sr_ctx* c) {
     R.table = c->table;
     dalloc(&c->held, n);
     dalloc(&c->push, 2 * n);
+    if (k.heat) {
+        dalloc(&c->radx, n);
+        dalloc(&c->rady, n);
+    }
     if (k.gravity) {
         dalloc(&c->src_free, n);
         dalloc(&c->phip, n);
@@ -256,8 +261,8 @@ static RefArgs ref_args(sr_ctx* c, int cur) {
     A.gym = c->gym;
     A.gxp = c->gxp;
     A.gyp = c->gyp;
-    A.radx = nullptr;  // the radiation force reads the last P5's flux; P5 is off in reference mode
-    A.rady = nullptr;
+    A.radx = c->radx;  // the last P5's cell-centred flux (zero before the first P5: no force), or none without P5
+    A.rady = c->rady;
     A.push = c->push;
     A.part = c->rpart;
     A.part_best = c->rbest;
@@ -350,6 +355,13 @@ static long long enqueue_step(sr_ctx* c, int cur, cudaStream_t s, cudaGraph_t ro
             mark(3);
         }
         mark(4);
+        if (k.heat) {
+            if (root) heat_top = heat_capture_step(c->heat, U, nullptr, &c->rec->dt, s, root);
+            else heat_step(c->heat, U, nullptr, &c->rec->dt, s, &c->heat_report);
+            const float *fx, *fy;
+            heat_flux_planes(c->heat, &fx, &fy);
+            ref_cell_flux_launch(fx, fy, c->radx, c->rady, c->w, c->h, s);
+        }
         mark(5);
         ref_floors_launch(c->R, U, s);
         ref_hold_dt_launch(c->R, U, c->held, k.gravity ? c->gx : nullptr, k.gravity ? c->gy : nullptr, 1, 1,
@@ -599,6 +611,16 @@ sr_status sr_create(const sr_config* cfg, sr_ctx** out) {
         dalloc(&c->part_g, (size_t)fb);
         dalloc(&c->part_nf, (size_t)fb);
         if (cfg->heat) c->heat = heat_create(*cfg, c->stream);
+        if (c->heat && ref_mode(c)) {
+            HeatRef hr;
+            hr.on = 1;
+            hr.table = c->table;
+            hr.cold_e = c->R.cold_e;
+            hr.cold_n = c->R.cold_n;
+            hr.kappa_dust = cfg->kappa_dust;
+            hr.t_dust = cfg->t_dust;
+            heat_set_reference(c->heat, hr);
+        }
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     } catch (const SrError& e) {
         g_create_error = e.message;
@@ -621,6 +643,10 @@ sr_status sr_upload(sr_ctx* c, const float* p, uint32_t nplanes) {
         SR_REQUIRE((int)nplanes == c->nc, "sr_upload: the context carries " + std::to_string(c->nc) + " planes");
         SR_CUDA_TRY(cudaMemcpyAsync(planes(c), p, sizeof(float) * c->nc * c->n, cudaMemcpyHostToDevice, c->stream));
         if (c->held) SR_CUDA_TRY(cudaMemsetAsync(c->held, 0, c->n, c->stream));  // a new state: none held yet
+        if (c->radx) {  // nor a flux: the first step takes no radiation force (reference/mod.rs:122-123)
+            SR_CUDA_TRY(cudaMemsetAsync(c->radx, 0, sizeof(float) * c->n, c->stream));
+            SR_CUDA_TRY(cudaMemsetAsync(c->rady, 0, sizeof(float) * c->n, c->stream));
+        }
         if (c->heat) heat_reset(c->heat, c->stream);
         initial_reductions(c);
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));

@@ -45,6 +45,7 @@ struct HeatConst {
     int w, h;
     double gm1, mu, t_floor, sigma_vac, sigma_floor, a_r, c_sb, kappa0, k_cond, chi;
     int limiter_on;
+    int ref;  // reference mode: the sides of heat_cells_kernel's reference branch (C = Σ/μ of each cell)
 };
 
 __device__ __forceinline__ double u_of(const HeatConst& K, double t) {
@@ -57,14 +58,68 @@ __device__ __forceinline__ double dt_du(const HeatConst& K, double t) {
     return K.chi > 0.0 ? 1.0 : 1.0 / (4.0 * K.a_r * ((t * t) * t));
 }
 
+// eos.rs:118-131 in f64 on the device tables (u at the node, Δ ln u to the next): u(x) = u_i exp(frac Δ_i)
+__device__ __forceinline__ double cold_u64(const float* u, const float* d, double x) {
+    if (!(x > 0.0)) return 0.0;
+    const double pos = (log(x) + 18.420680743952367) * (511.0 / 36.841361487904734);
+    if (pos < 0.0) {
+        const double r = x * 1e8;
+        return (double)u[0] * r * r;
+    }
+    int i = (int)pos;
+    i = i > 510 ? 510 : i;
+    return (double)u[i] * exp((pos - (double)i) * (double)d[i]);
+}
+
 // ---- step set-up: the sides (heat.rs:215-226), the faces' D_f (heat.rs:263-294), Σ_f k and its vacuum part
-__global__ void heat_cells_kernel(HeatConst K, const float* __restrict__ U, const float* __restrict__ kappa,
+__global__ void heat_cells_kernel(HeatConst K, HeatRef RF, const float* __restrict__ U, const float* __restrict__ kappa,
                                   uint8_t* gas, double* t0, double* C, float* kap, float* sig, double* t, double* u,
                                   Red R) {
     const size_t n = (size_t)K.w * K.h;
     double acc = 0.0, ngas = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         const double s = U[i];
+        if (RF.on) {
+            // reference/heat.rs:215-231 with the registry's composition (registry.rs:145-154)
+            const double za[10] = {2.0, 0.75, 7.0 / 12.0, 9.0 / 16.0, 11.0 / 20.0, 13.0 / 24.0, 15.0 / 28.0,
+                                   17.0 / 32.0, 27.0 / 56.0, 1.0};
+            const double ze[10] = {1.0, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 0.5, 26.0 / 56.0, 0.0};
+            double inv_mu = 0.0, ye = 0.0, x0 = 0.0, x1 = 0.0, xn = 0.0;
+            for (int k = 0; k < 10; k++) {
+                const double x = U[(4 + k) * n + i];
+                inv_mu += x * za[k];
+                ye += x * ze[k];
+                if (k == 0) x0 = x;
+                if (k == 1) x1 = x;
+                if (k == 9) xn = x;
+            }
+            const double mu = 1.0 / inv_mu, z_met = 1.0 - x0 - x1 - xn;
+            double T;
+            const bool g = s >= K.sigma_vac;
+            if (!g) {
+                T = K.t_floor;
+            } else {
+                const double mx = U[n + i], my = U[2 * n + i], e = U[3 * n + i];
+                double cold = 0.0;
+                if (RF.cold_e) cold += cold_u64(RF.table, RF.table + 512, ye * s);
+                if (RF.cold_n) cold += cold_u64(RF.table + 1024, RF.table + 1536, xn * s);
+                const double raw = e / s - 0.5 * (mx * mx + my * my) / (s * s) - cold / s;
+                const double floor = K.t_floor / mu;
+                T = mu * (raw < floor ? floor : raw);
+            }
+            kap[i] = (float)(K.kappa0 * (1.0 + x0) + (T < RF.t_dust ? RF.kappa_dust * z_met : 0.0));
+            gas[i] = g ? 1 : 0;
+            t0[i] = T;
+            sig[i] = g ? (float)s : (float)K.sigma_floor;
+            C[i] = (g ? s : K.sigma_floor) * inv_mu;
+            t[i] = T;
+            u[i] = u_of(K, T);
+            if (g) {
+                acc += C[i] * T;
+                ngas += 1.0;
+            }
+            continue;
+        }
         const float k = kappa ? kappa[i] : (float)K.kappa0;
         kap[i] = k;
         if (s < K.sigma_vac) {
@@ -117,7 +172,7 @@ __device__ __forceinline__ Side vacuum_beyond(const HeatConst& K, const Side& g)
     o.t = K.t_floor;
     o.s = K.sigma_floor;
     o.kappa = g.kappa;
-    o.c = K.sigma_floor / (K.mu * K.gm1);
+    o.c = K.ref ? K.sigma_floor * (g.c / g.s) : K.sigma_floor / (K.mu * K.gm1);  // the gas side's μ
     return o;
 }
 
@@ -1010,6 +1065,7 @@ struct RoundGraph {
 struct HeatSolver {
     sr_config cfg{};
     HeatConst K{};
+    HeatRef ref{};
     int w = 0, h = 0;
     size_t n = 0;
     int grid = 0;
@@ -1068,7 +1124,7 @@ void set_scalar(HeatSolver* H, int slot, double value, cudaStream_t s) {
 
 void setup_step(HeatSolver* H, const float* U, const float* kappa, cudaStream_t s) {
     const HeatConst& K = H->K;
-    heat_cells_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, U, kappa, H->gas, H->t0, H->C, H->kap, H->sig, H->t, H->u,
+    heat_cells_kernel<<<H->grid, RED_THREADS, 0, s>>>(K, H->ref, U, kappa, H->gas, H->t0, H->C, H->kap, H->sig, H->t, H->u,
                                                       H->red(S_HEAT0));
     sr_note_launch();
     const size_t nf = (size_t)(H->w + 1) * H->h + (size_t)H->w * (H->h + 1);
@@ -1614,6 +1670,17 @@ int heat_collect(HeatSolver* H, Learner* L, const float* U, const float* kappa, 
 }
 
 void heat_reset(HeatSolver* H, cudaStream_t s) { SR_CUDA_TRY(cudaMemsetAsync(H->rate, 0, sizeof(double) * H->n, s)); }
+
+void heat_set_reference(HeatSolver* H, const HeatRef& R) {
+    H->ref = R;
+    H->K.ref = R.on;
+    drop_step_graphs(H);
+}
+
+void heat_flux_planes(const HeatSolver* H, const float** fx, const float** fy) {
+    *fx = H->fx;
+    *fy = H->fy;
+}
 
 void heat_set_limits(HeatSolver* H, uint32_t max_passes, uint32_t max_rounds) {
     H->max_passes = max_passes;

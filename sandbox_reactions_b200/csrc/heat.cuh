@@ -6,7 +6,20 @@
 
 struct HeatSolver;
 
+// Reference mode's sides (reference/heat.rs:215-231): T from the reference's EOS (the cold energy of the K pairs'
+// tables taken off), C = Σ/μ and κ = κ₀(1 + X_H) (+ κ_dust Z_met below T_dust) of each cell's species, read from the
+// 14-plane state.
+struct HeatRef {
+    int on = 0;
+    const float* table = nullptr;  // device: u_e, Δ ln u_e, u_n, Δ ln u_n at the 512 nodes
+    int cold_e = 0, cold_n = 0;
+    double kappa_dust = 0.0, t_dust = 0.0;
+};
+
 HeatSolver* heat_create(const sr_config& cfg, cudaStream_t s);
+void heat_set_reference(HeatSolver* hs, const HeatRef& R);
+// The last step's face fluxes on the device ((W+1)*H and W*(H+1) floats).
+void heat_flux_planes(const HeatSolver* hs, const float** fx, const float** fy);
 void heat_destroy(HeatSolver* hs);
 // One implicit step of length *dt_dev on the 4 planes U (E changes), κ from `kappa` (W*H) or cfg.kappa0.
 void heat_step(HeatSolver* hs, float* U, const float* kappa, const double* dt_dev, cudaStream_t s, sr_heat_report* rep);

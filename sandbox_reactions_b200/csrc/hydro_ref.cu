@@ -1015,6 +1015,16 @@ __global__ void ref_hold_dt_kernel(RefConst R, float* __restrict__ U, uint8_t* _
     }
 }
 
+__global__ void ref_cell_flux_kernel(const float* __restrict__ fx, const float* __restrict__ fy, float* radx, float* rady,
+                                     int w, int h) {
+    const size_t n = (size_t)w * h;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t x = i % w, y = i / w;
+        radx[i] = 0.5f * (fx[y * (w + 1) + x] + fx[y * (w + 1) + x + 1]);
+        rady[i] = 0.5f * (fy[y * w + x] + fy[(y + 1) * w + x]);
+    }
+}
+
 int ref_grid(size_t n) {
     const size_t b = (n + 255) / 256;
     return (int)(b < 1 ? 1 : (b > 148 * 8 ? 148 * 8 : b));
@@ -1106,6 +1116,11 @@ void ref_hydro_finalize_launch(const RefArgs& A, cudaStream_t s) {
     ref_reduce_kernel<<<1, 256, 0, s>>>(A, ref_hydro_blocks(A.R.w, A.R.h));
     sr_note_launch();
     ref_apply_kernel<<<ref_grid((size_t)A.R.w * A.R.h), 256, 0, s>>>(A);
+    sr_note_launch();
+}
+
+void ref_cell_flux_launch(const float* fx, const float* fy, float* radx, float* rady, int w, int h, cudaStream_t s) {
+    ref_cell_flux_kernel<<<ref_grid((size_t)w * h), 256, 0, s>>>(fx, fy, radx, rady, w, h);
     sr_note_launch();
 }
 

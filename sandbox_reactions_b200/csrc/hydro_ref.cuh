@@ -54,6 +54,10 @@ void ref_hydro_update_launch(const RefArgs& A, int gravity, cudaStream_t s);
 // The take-backs (the radiation force's net push, gravity's net kick) and the sticky wall on the updated state.
 void ref_hydro_finalize_launch(const RefArgs& A, cudaStream_t s);
 
+// The cell-centred flux the next step's radiation force reads: the mean of a cell's two faces on each axis
+// (reference/heat.rs:100-112).
+void ref_cell_flux_launch(const float* fx, const float* fy, float* radx, float* rady, int w, int h, cudaStream_t s);
+
 // P8's floors (floors.rs:124-175) in place.
 void ref_floors_launch(const RefConst& R, float* U, cudaStream_t s);
 // The hold (floors.rs:196-243) and/or P9's per-CTA Δt terms with the 14-channel guard; then, with `do_dt`, the

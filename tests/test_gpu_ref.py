@@ -10,7 +10,12 @@ C ABI against the oracle's reference-mode twin (oracle/sr_oracle_ref.c; referenc
   - a cold disk under the shipped physics (the cold pairs on, gravity, leave edges): 3 steps;
   - a dense cold core the hold's rule holds, with gravity: 4 steps — the held cells behind their reflecting walls, the
     pull on them from the free cells' field, the sticky wall; the mask equal to the twin's after every step;
-  - the hold's mask through sr_upload_held / sr_read_held."""
+  - the hold's mask through sr_upload_held / sr_read_held;
+  - reference-mode P5 (C = Σ/μ, T from the EOS with the cold energy, κ of the species) on scenes/heat_ceiling.bin and
+    heat_overflow.bin: the reference's own GPU check of the cut (converged, |δ| <= 1e-5, no cell losing more than the
+    heat it holds, the grid losing what it books) and T against the converged twin (C-weighted L1 <= 1e-4);
+  - four full reference-mode steps with heat on a hot disk: P2, P4 with the radiation force of the last P5's flux, P5,
+    P8 and the hold, P9."""
 import os
 
 import numpy as np
@@ -176,3 +181,84 @@ def test_the_hold_mask_round_trips():
         m = (rng.random((cfg.height, cfg.width)) < 0.1).astype(np.uint32)
         s.upload_held(m)
         assert np.array_equal(s.read_held(), m)
+
+
+def heat_gap(cfg, before, gpu, ref):
+    """heat.rs:1360-1367's measures: the GPU's T against the twin's, C-weighted relative L1 (C = Σ/μ of the start) and
+    the worst cell with Σ >= 1e-4."""
+    tg = O.ref_heat_sides(cfg, gpu.astype(np.float64))[0]
+    tt = O.ref_heat_sides(cfg, ref)[0]
+    _, _, inv_mu = O.ref_heat_sides(cfg, before.astype(np.float64))
+    c = before[0].astype(np.float64) * inv_mu
+    l1 = (c * np.abs(tg - tt)).sum() / (c * tt).sum()
+    sel = before[0] >= 1e-4
+    cell = (np.abs(tg - tt) / tt)[sel].max()
+    return l1, cell
+
+
+@pytest.mark.parametrize("name", ["heat_ceiling", "heat_overflow"])
+def test_the_reference_heat_cuts_step_like_the_converged_twin(name):
+    # scenes/heat_ceiling.bin and heat_overflow.bin (tests/golden/*.npz): P5 at the cut's own Δt on a_r 4e-5, c_sb 200
+    # (crates/sr-engine/tests/gpu/heat.rs:1413-1437), then P8. The reference's own GPU check of the ceiling cut
+    # (heat.rs:1534-1566): the step converges in under 64 passes and 4,096 rounds, |δ| <= 1e-5, and no gas cell loses
+    # more than the heat it holds above its floor, the grid losing what it books (1e-5 of that heat). Beside it, against
+    # the twin run to convergence (its 4,096-round ceiling lifted: 16 passes / 5,065 rounds and 22 / 10,019 at the
+    # twin's 1e-12 tolerances): T's C-weighted L1 <= 1e-4 (the one-pass bar, heat.rs:1385), every cell with Σ >= 1e-4
+    # within 5e-3 — the device's Newton stop (the reference GPU's rule) ends a step once no cell's T moved by more than
+    # 1e-3 of itself in the last pass, so a cell may sit that far from the converged answer (measured 1.7e-3 on the
+    # ceiling cut, 9e-7 in L1)
+    f = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    P = f["planes"]
+    dt = float(np.float32(f["dt_next"]))
+    cfg = Config(width=64, height=64, channels=14, heat=True, hydro=False, gravity=False, a_r=4e-5, c_sb=200.0,
+                 dt_fixed=dt)
+    with Step(cfg) as s:
+        s.upload(P)
+        s.run(1)
+        gpu = s.readback()
+        rep = s.read_heat()
+    assert rep.converged and rep.passes < 64 and rep.rounds < 4096, (rep.passes, rep.rounds)
+    assert abs(rep.delta) <= 1e-5, rep.delta
+    P64, G64 = P.astype(np.float64), gpu.astype(np.float64)
+    t0, _, inv_mu = O.ref_heat_sides(cfg, P64)
+    gas = P64[0] >= cfg.sigma_vac
+    held = np.where(gas, P64[0] * inv_mu * (t0 - cfg.t_floor), 0.0)
+    lost = P64[3] - G64[3]
+    eps32 = 2.0 * float(np.finfo(np.float32).eps)
+    assert np.all(lost[gas] <= held[gas] * (1 + 1e-5) + eps32 * np.abs(P64[3][gas]))
+    assert abs(lost.sum() - rep.radiated) <= 1e-5 * held.sum(), (lost.sum(), rep.radiated)
+    assert rep.radiated <= held.sum() * (1 + 1e-5)
+    twin = O.RefTwin(cfg.replace(max_rounds=200000), P64)
+    twin.step()
+    ref, _ = twin.state()
+    trep, _, _ = twin.heat()
+    assert trep.converged
+    l1, cell = heat_gap(cfg, P, gpu, ref)
+    assert l1 <= 1e-4 and cell <= 5e-3, (l1, cell)
+    assert abs(rep.radiated - trep.radiated) <= 1e-3 * trep.radiated, (rep.radiated, trep.radiated)
+    assert np.array_equal(gpu[0], P[0]) or np.abs(gpu[0] - P[0]).max() <= 1e-7 * np.abs(P[0]).max()
+
+
+HOT_DISK = """{"version": 1,
+ "world": {"width": 96, "height": 96, "edge": "leave"},
+ "slowdown": false,
+ "switches": {"gravity": true, "hydro": true, "heat": true, "reactions": false, "neutrinos": false, "sinks": false},
+ "objects": [
+   {"kind": "rect", "x0": 0, "y0": 0, "w": 96, "h": 96, "sigma": 2e-3, "t": 1.0, "composition": {"H": 1.0},
+    "v": [0, 0]},
+   {"kind": "disk", "x": 48, "y": 48, "a": 30, "sigma_c": 1.0, "t": 40.0,
+    "composition": {"H": 0.7346, "He": 0.2485, "C": 0.0092, "O": 0.0077}, "v": [0.05, 0.02]},
+   {"kind": "disk", "x": 40, "y": 52, "a": 6, "sigma_c": 2.0, "t": 400.0, "composition": {"He": 1.0}, "v": [0, 0]}
+ ]}"""
+
+
+def test_a_full_reference_step_with_heat_and_the_radiation_force_steps_like_the_twin():
+    # P2, P4 (the radiation force of the last P5's F from the second step on), P5 (C = Σ/μ and κ = κ₀(1 + X_H) of each
+    # cell's species, T from the EOS with the shipped cold pressures), P8 and the hold, P9: four steps
+    sc = Scene.parse(HOT_DISK)
+    P, _ = sc.planes()
+    cfg = sc.ref_config(strict=False).replace(heat=True)
+    outs, _, clock, touts, _, twin = run_both(cfg, P, 4)
+    for k in range(4):
+        compare(outs[k], touts[k], 2e-5, f"step {k + 1}")
+    assert abs(clock.sim_time - twin.clock()["sim_time"]) <= 1e-5 * twin.clock()["sim_time"]

@@ -11,7 +11,11 @@ against the reference's known answers:
     cell leaves at |v| ~ 2,100, 54.6x its neighbours' (the figures the reference test's comments give);
   - with the cold pairs off and one species, reference mode steps the same gas as the config-mode oracle at γ = 2 and
     that species' μ (two code paths, one answer);
-  - P8's floors and the hold on hand-made cells (floors.rs:124-243)."""
+  - P8's floors and the hold on hand-made cells (floors.rs:124-243);
+  - reference-mode P5 on scenes/heat_ceiling.bin (tests/golden/heat_ceiling.npz): the twin's step reaches the ceiling
+    in 11 passes and 4,096 rounds and commits by limited fluxes with δ = 0 within the bounds to 1e-9 (the known answer
+    crates/sr-engine/tests/gpu/heat.rs:1486-1501 states); with one species and no cold pressure it is the config-mode
+    step with that μ and κ₀(1 + X_H)."""
 import math
 import os
 
@@ -205,3 +209,54 @@ def test_floors_and_the_hold_on_hand_made_cells():
     # the disk gate: the same cell inside a disk of more than m_tov is free
     _, m4, _ = O.ref_hold(cfg.replace(m_tov=10.0), Q, held=m)
     assert m4[8, 8] == 0
+
+
+def heat_cut(name):
+    f = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    # the cuts ran on a_r 4e-5 and c_sb 200 (crates/sr-engine/tests/gpu/heat.rs:1433-1437), every test flag off
+    cfg = Config(width=64, height=64, channels=14, heat=True, hydro=False, gravity=False, a_r=4e-5, c_sb=200.0)
+    return cfg, f["planes"].astype(np.float64), float(np.float32(f["dt_next"]))
+
+
+def held_above_floor(cfg, P):
+    """heat.rs tests' held_above_floor: C (T⁰ - T_floor) on the gas, 0 off it."""
+    t0, _, inv_mu = O.ref_heat_sides(cfg, P)
+    gas = P[0] >= cfg.sigma_vac
+    return np.where(gas, P[0] * inv_mu * (t0 - cfg.t_floor), 0.0)
+
+
+def test_the_ceiling_cut_reaches_the_ceiling_and_moves_no_more_heat_than_its_cells_hold():
+    # heat.rs:1486-1501: the twin's step of scenes/heat_ceiling.bin reaches the ceiling in 11 passes and 4,096 rounds;
+    # its commit by limited fluxes has δ = 0 and holds the bounds to 1e-9
+    cfg, P, dt = heat_cut("heat_ceiling")
+    out, rep, _, _ = O.ref_heat_step(cfg, P, dt)
+    assert (rep.passes, rep.rounds, rep.converged, rep.delta) == (11, 4096, 0, 0.0)
+    held = held_above_floor(cfg, P)
+    lost = P[3] - out[3]
+    gas = P[0] >= cfg.sigma_vac
+    assert np.all(lost[gas] <= held[gas] * (1 + 1e-9) + 1e-12 * np.abs(P[3][gas]))
+    assert abs(lost.sum() - rep.radiated) <= 1e-9 * held.sum()
+    assert rep.radiated <= held.sum() * (1 + 1e-9)
+
+
+def test_reference_mode_heat_with_one_species_is_the_config_mode_step():
+    # C = Σ/μ, T = μ ε_th and κ = κ₀(1 + X_H) of one species and no cold pressure: the config-mode step at γ = 2 with
+    # that μ and the κ plane κ₀(1 + X_H)
+    rng = np.random.default_rng(11)
+    h, w = 32, 40
+    s = 0.5 + rng.random((h, w))
+    s[:4, :] = 1e-9
+    e = s * (1.0 + 4.0 * rng.random((h, w)))
+    P = np.zeros((14, h, w))
+    P[0], P[3] = s, e
+    P[4], P[5] = 0.7, 0.3
+    off = dict(k1e=0.0, k2e=0.0, k1n=0.0, k2n=0.0)
+    cfg = Config(width=w, height=h, channels=14, heat=True, hydro=False, **off)
+    out, rep, fx, fy = O.ref_heat_step(cfg, P, 0.05)
+    inv_mu = O.composition([0.7, 0.3] + [0.0] * 8)[0]
+    c4 = cfg.replace(channels=4, mu=1.0 / inv_mu, gamma=2.0, opacity_plane=True)
+    kappa = np.full((h, w), cfg.kappa0 * 1.7)
+    o4, r4, fx4, fy4 = O.heat_step(c4, P[:4], 0.05, kappa)
+    assert rep.converged and r4.converged and rep.passes == r4.passes
+    assert np.abs(out[3] - o4[3]).max() <= 1e-10 * np.abs(o4[3]).max()
+    assert np.abs(fx - fx4).max() <= 1e-10 * np.abs(fx4).max()
