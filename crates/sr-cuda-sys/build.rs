@@ -9,7 +9,7 @@ use std::path::{Path, PathBuf};
 use std::process::Command;
 
 const SOURCES: &[&str] = &[
-    "ctx.cu", "hydro.cu",
+    "ctx.cu", "box.cu", "hydro.cu",
     "hydro_ref.cu", "grav.cu", "grav_static.cu", "heat.cu", "mg.cu", "batch.cu", "learned.cu",
 ];
 

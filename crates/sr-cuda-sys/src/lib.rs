@@ -54,7 +54,8 @@ pub struct sr_config {
     pub max_passes: u32,
     pub max_rounds: u32,
     pub pin_temperature: u32,
-    pub reserved: [u32; 4],
+    pub active_box: u32,
+    pub reserved: [u32; 3],
     pub gamma: f64,
     pub mu: f64,
     pub t_floor: f64,
@@ -118,6 +119,18 @@ pub struct sr_heat_report {
 
 #[repr(C)]
 #[derive(Clone, Copy, Debug, Default)]
+pub struct sr_box_report {
+    pub x0: u32,
+    pub y0: u32,
+    pub w: u32,
+    pub h: u32,
+    pub fft_w: u32,
+    pub fft_h: u32,
+    pub fits: u64,
+}
+
+#[repr(C)]
+#[derive(Clone, Copy, Debug, Default)]
 pub struct sr_cost {
     pub steps: u32,
     pub pad: u32,
@@ -154,6 +167,7 @@ extern "C" {
     pub fn sr_upload(ctx: *mut sr_ctx, planes: *const f32, nplanes: u32) -> sr_status;
     pub fn sr_readback(ctx: *mut sr_ctx, planes: *mut f32, nplanes: u32) -> sr_status;
     pub fn sr_upload_held(ctx: *mut sr_ctx, mask: *const u32) -> sr_status;
+    pub fn sr_read_box(ctx: *mut sr_ctx, out: *mut sr_box_report) -> sr_status;
     pub fn sr_read_held(ctx: *mut sr_ctx, mask: *mut u32) -> sr_status;
     pub fn sr_upload_opacity(ctx: *mut sr_ctx, kappa: *const f32) -> sr_status;
     pub fn sr_step(ctx: *mut sr_ctx, steps: u32) -> sr_status;

@@ -75,7 +75,11 @@ typedef struct sr_config {
     uint32_t max_passes;      /* Newton passes per implicit step (reference heat.rs:51 MAX_PASSES = 128) */
     uint32_t max_rounds;      /* PCG rounds over all passes (heat.rs:52 MAX_ROUNDS = 4096) */
     uint32_t pin_temperature; /* heat.rs TestFlags::pin_temperature */
-    uint32_t reserved[4];
+    uint32_t active_box;      /* 1: the active box (crates/sr-engine/src/step/boxfit.rs, BoxMode::Fit): only the bounding
+                                 box of the cells with Σ >= Σ_vac, grown by 8 and rounded out to multiples of 8, is
+                                 stepped, its FFT sized to it, refit before step 0 and after every 16th step's P9; the
+                                 vacuum outside is left as it is. 0: the whole world (BoxMode::WholeWorld) */
+    uint32_t reserved[3];
     double gamma;             /* adiabatic index: Π = (γ-1) Σ ε_th, c² = γΠ/Σ (the reference hardwires γ = 2) */
     double mu;                /* mean molecular weight: T = μ (γ-1) ε_th (the reference's T = μ ε_th at γ = 2) */
     double t_floor;           /* physics.json t_floor */
@@ -194,6 +198,16 @@ sr_status sr_set_edge_mode(sr_ctx* ctx, uint32_t edge);
 sr_status sr_set_heat_precond(sr_ctx* ctx, uint32_t precond);
 /* Step::set_heat_rounds (step/heat.rs:529-533): the ceilings of the implicit step. */
 sr_status sr_set_heat_limits(sr_ctx* ctx, uint32_t max_passes, uint32_t max_rounds);
+/* BoxFit::read (crates/sr-engine/src/step/boxfit.rs:33-53, 152-172): the active box as it stands — origin and size
+ * in cells (the whole world when the box is off or no cell holds gas), the FFT size per axis the step's gravity runs
+ * on, and the fits made since the upload. */
+typedef struct sr_box_report {
+    uint32_t x0, y0, w, h;
+    uint32_t fft_w, fft_h;
+    uint64_t fits;
+} sr_box_report;
+sr_status sr_read_box(sr_ctx* ctx, sr_box_report* out);
+
 /* Step::set_timing / read_cost (step/mod.rs:722-777). `on`: 0 off; 1 each step's device time (total_ms) as the steps
  * normally run — after the first step, one captured graph per step — with the per-pass fields left 0; 2 the per-pass
  * breakdown, the passes launched one by one (the implicit step still one captured graph after the first step). */

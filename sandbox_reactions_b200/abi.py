@@ -27,7 +27,7 @@ class sr_config(C.Structure):
         ("gravity", C.c_uint32), ("hydro", C.c_uint32), ("heat", C.c_uint32),
         ("kernel", C.c_uint32), ("precond", C.c_uint32), ("flux_limiter", C.c_uint32), ("opacity_plane", C.c_uint32),
         ("mg_pre", C.c_uint32), ("mg_post", C.c_uint32), ("max_passes", C.c_uint32), ("max_rounds", C.c_uint32),
-        ("pin_temperature", C.c_uint32), ("reserved", C.c_uint32 * 4),
+        ("pin_temperature", C.c_uint32), ("active_box", C.c_uint32), ("reserved", C.c_uint32 * 3),
         ("gamma", C.c_double), ("mu", C.c_double), ("t_floor", C.c_double), ("sigma_vac", C.c_double),
         ("sigma_floor", C.c_double), ("cfl", C.c_double), ("eta_g", C.c_double), ("G", C.c_double),
         ("softening", C.c_double), ("a_r", C.c_double), ("c_sb", C.c_double), ("kappa0", C.c_double),
@@ -49,6 +49,11 @@ class sr_heat_report(C.Structure):
     _fields_ = [("dt", C.c_double), ("passes", C.c_uint32), ("rounds", C.c_uint32), ("refinements", C.c_uint32),
                 ("converged", C.c_uint32), ("delta", C.c_double), ("radiated", C.c_double),
                 ("rel_residual", C.c_double), ("fallback_used", C.c_uint32), ("precond", C.c_uint32)]
+
+
+class sr_box_report(C.Structure):
+    _fields_ = [("x0", C.c_uint32), ("y0", C.c_uint32), ("w", C.c_uint32), ("h", C.c_uint32), ("fft_w", C.c_uint32),
+                ("fft_h", C.c_uint32), ("fits", C.c_uint64)]
 
 
 class sr_cost(C.Structure):
@@ -79,6 +84,7 @@ class Config:
     max_passes: int = 128
     max_rounds: int = 4096
     pin_temperature: bool = False
+    active_box: bool = False    # step only the box around the gas (the reference's BoxMode::Fit); False: the whole world
     gamma: float = 2.0
     mu: float = 1.0
     t_floor: float = 0.05

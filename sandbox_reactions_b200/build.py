@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsrcuda.so")
-SOURCES = ["ctx.cu", "hydro.cu", "hydro_ref.cu", "grav.cu", "grav_static.cu", "heat.cu", "mg.cu", "batch.cu", "learned.cu"]
+SOURCES = ["ctx.cu", "box.cu", "hydro.cu", "hydro_ref.cu", "grav.cu", "grav_static.cu", "heat.cu", "mg.cu", "batch.cu", "learned.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]

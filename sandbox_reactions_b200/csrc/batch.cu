@@ -142,6 +142,12 @@ sr_status sr_batch_create(const sr_config* cfgs, uint32_t count, uint32_t thread
     sr_batch* b = new sr_batch();
     std::vector<size_t> cells;
     for (uint32_t i = 0; i < count; i++) {
+        if (cfgs[i].active_box) {  // a batch step is one graph over its worlds' whole steps: their boxes would refit
+            sr_batch_destroy(b);
+            sr_set_global_error("world " + std::to_string(i) + ": the active box is a single world's (batch worlds "
+                                "step whole)");
+            return SR_E_UNSUPPORTED;
+        }
         sr_ctx* c = nullptr;
         sr_status st = sr_create(&cfgs[i], &c);
         if (st != SR_OK) {

@@ -5,10 +5,12 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <functional>
 #include <string>
 #include <vector>
 
+#include "box.cuh"
 #include "grav.cuh"
 #include "heat.cuh"
 #include "hydro.cuh"
@@ -72,6 +74,15 @@ struct sr_ctx {
     cudaGraphExec_t step_graph[2] = {nullptr, nullptr};  // a whole step from state buffer 0 / 1, captured on first use
     long long step_launches = 0;
     unsigned generation = 0;  // counts the invalidations of captured steps (a batch's graph checks it)
+    // the active box: the crop of the world's gas stepped as a world of its own (a context per box size met)
+    bool use_box = false;
+    BoxRec box{};                 // the box `sub` steps
+    sr_ctx* sub = nullptr;        // the crop's context while the box is active
+    std::vector<sr_ctx*> subs;    // the crop contexts made so far (owned)
+    int* box_part = nullptr;      // the fit's per-CTA partials
+    int* box_rec = nullptr;       // the fitted box (device)
+    unsigned long long box_steps = 0;  // steps since the upload: the refit cadence
+    unsigned long long box_fits = 0;
     // timing
     int timing = 0;  // 0 off; 1 each step's device time (captured steps); 2 per pass (passes launched one by one)
     std::vector<cudaEvent_t> events;
@@ -139,6 +150,8 @@ static void drop_step_graphs(sr_ctx* c) {
         }
 }
 
+static void ctx_free(sr_ctx* c);
+
 static void ctx_free(sr_ctx* c) {
     if (!c) return;
     if (c->stream) cudaStreamSynchronize(c->stream);
@@ -147,6 +160,8 @@ static void ctx_free(sr_ctx* c) {
     cudaFree(c->phi); cudaFree(c->gx); cudaFree(c->gy);
     cudaFree(c->src); cudaFree(c->phim); cudaFree(c->gxm); cudaFree(c->gym);
     cudaFree(c->kappa);
+    for (sr_ctx* s : c->subs) ctx_free(s);
+    cudaFree(c->box_part); cudaFree(c->box_rec);
     cudaFree(c->table); cudaFree(c->held); cudaFree(c->src_free); cudaFree(c->phip); cudaFree(c->gxp);
     cudaFree(c->gyp); cudaFree(c->push); cudaFree(c->radx); cudaFree(c->rady); cudaFree(c->rpart); cudaFree(c->rbest); cudaFree(c->ridx); cudaFree(c->rfin);
     if (c->grav_ready) c->grav.destroy();
@@ -429,6 +444,145 @@ void sr_ctx_graph_steps_done(sr_ctx* c, uint32_t steps, long long launches_per_s
     sr_note_launches(launches_per_step * (long long)steps);
 }
 
+// ---- the active box (crates/sr-engine/src/step/boxfit.rs): the crop of the world around its gas, stepped as a world
+// of its own. Cells outside the box hold vacuum that no pass changes (the reference's box passes leave it alone), and
+// with 8 cells of vacuum inside the box's edge the crop's edge cells are empty, so its edge mode changes no flux; its
+// FFT is sized to the box, as the reference's is.
+
+// Copies `count` planes of the box's cells between the world (W x H planes) and a crop (bw x bh planes).
+static void box_copy(void* dst, int dst_pitch, size_t dst_plane, const void* src, int src_pitch, size_t src_plane,
+                     int count, int bw, int bh, size_t elem, cudaStream_t s) {
+    for (int k = 0; k < count; k++)
+        SR_CUDA_TRY(cudaMemcpy2DAsync((char*)dst + k * dst_plane * elem, dst_pitch * elem,
+                                      (const char*)src + k * src_plane * elem, src_pitch * elem, bw * elem, bh,
+                                      cudaMemcpyDeviceToDevice, s));
+}
+
+// The world's cells of the box into the crop context `s` (its planes and what the next step reads beside them).
+static void crop_in(sr_ctx* c, sr_ctx* s, const BoxRec& b, bool with_record) {
+    SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const size_t off = (size_t)b.y0 * c->w + b.x0;
+    box_copy(s->U[s->cur], b.w, s->n, planes(c) + off, c->w, c->n, c->nc, b.w, b.h, sizeof(float), s->stream);
+    if (c->kappa) box_copy(s->kappa, b.w, s->n, c->kappa + off, c->w, c->n, 1, b.w, b.h, sizeof(float), s->stream);
+    if (c->held) box_copy(s->held, b.w, s->n, c->held + off, c->w, c->n, 1, b.w, b.h, 1, s->stream);
+    if (c->radx) {
+        box_copy(s->radx, b.w, s->n, c->radx + off, c->w, c->n, 1, b.w, b.h, sizeof(float), s->stream);
+        box_copy(s->rady, b.w, s->n, c->rady + off, c->w, c->n, 1, b.w, b.h, sizeof(float), s->stream);
+    }
+    if (c->heat && s->heat)
+        box_copy(heat_rate_plane(s->heat), b.w, s->n, heat_rate_plane(c->heat) + off, c->w, c->n, 1, b.w, b.h,
+                 sizeof(double), s->stream);
+    if (with_record) SR_CUDA_TRY(cudaMemcpyAsync(s->rec, c->rec, sizeof(DtRecord), cudaMemcpyDeviceToDevice, s->stream));
+    s->uploaded = true;
+}
+
+// The crop's cells back into the world, and its Δt record (the guard's cell in world coordinates).
+static void crop_out(sr_ctx* c, sr_ctx* s, const BoxRec& b) {
+    SR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    const size_t off = (size_t)b.y0 * c->w + b.x0;
+    box_copy(planes(c) + off, c->w, c->n, s->U[s->cur], b.w, s->n, c->nc, b.w, b.h, sizeof(float), c->stream);
+    if (c->held) box_copy(c->held + off, c->w, c->n, s->held, b.w, s->n, 1, b.w, b.h, 1, c->stream);
+    if (c->radx) {
+        box_copy(c->radx + off, c->w, c->n, s->radx, b.w, s->n, 1, b.w, b.h, sizeof(float), c->stream);
+        box_copy(c->rady + off, c->w, c->n, s->rady, b.w, s->n, 1, b.w, b.h, sizeof(float), c->stream);
+    }
+    if (c->heat && s->heat)
+        box_copy(heat_rate_plane(c->heat) + off, c->w, c->n, heat_rate_plane(s->heat), b.w, s->n, 1, b.w, b.h,
+                 sizeof(double), c->stream);
+    DtRecord rec;
+    SR_CUDA_TRY(cudaMemcpyAsync(&rec, s->rec, sizeof rec, cudaMemcpyDeviceToHost, c->stream));
+    SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (rec.non_finite)
+        rec.nf_cell = (rec.nf_cell / b.w + b.y0) * (long long)c->w + rec.nf_cell % b.w + b.x0;
+    SR_CUDA_TRY(cudaMemcpyAsync(c->rec, &rec, sizeof rec, cudaMemcpyHostToDevice, c->stream));
+    SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+}
+
+// The box of the state as it stands: over the crop while one is stepped (the vacuum outside it holds no gas).
+static BoxRec fit_box(sr_ctx* c) {
+    const float* sig = c->sub ? c->sub->U[c->sub->cur] : planes(c);
+    const int w = c->sub ? c->sub->w : c->w, h = c->sub ? c->sub->h : c->h;
+    const int ox = c->sub ? c->box.x0 : 0, oy = c->sub ? c->box.y0 : 0;
+    cudaStream_t st = c->sub ? c->sub->stream : c->stream;
+    box_fit_launch(sig, w, h, ox, oy, c->w, c->h, (float)c->cfg.sigma_vac, c->box_part, c->box_rec, st);
+    int r[4];
+    SR_CUDA_TRY(cudaMemcpyAsync(r, c->box_rec, sizeof r, cudaMemcpyDeviceToHost, st));
+    SR_CUDA_TRY(cudaStreamSynchronize(st));
+    c->box_fits++;
+    BoxRec b{r[0], r[1], r[2], r[3]};
+    if (b.w == 0 || b.h == 0) b = BoxRec{0, 0, c->w, c->h};  // no gas: the whole world runs the step
+    return b;
+}
+
+// The crop context for a box of this size (made on first use, kept for the boxes that follow).
+static sr_ctx* sub_for(sr_ctx* c, int w, int h) {
+    for (sr_ctx* s : c->subs)
+        if (s->w == w && s->h == h) return s;
+    sr_config k = c->cfg;
+    k.width = (uint32_t)w;
+    k.height = (uint32_t)h;
+    k.active_box = 0;
+    sr_ctx* s = nullptr;
+    const sr_status st = sr_create(&k, &s);
+    if (st != SR_OK) throw SrError{st, "the active box's context: " + g_create_error};
+    s->timing = c->timing;
+    if (c->learner && s->heat) {
+        heat_attach_learned(s->heat, c->learner->L);
+        s->learner = c->learner;
+    }
+    c->subs.push_back(s);
+    return s;
+}
+
+// A refit (reference: before step 0, and after P9 at step indices ≡ 0 mod 16): the crop follows the gas.
+static void refit(sr_ctx* c) {
+    const BoxRec b = fit_box(c);
+    if (c->sub && b.x0 == c->box.x0 && b.y0 == c->box.y0 && b.w == c->box.w && b.h == c->box.h) return;
+    if (c->sub) crop_out(c, c->sub, c->box);
+    sr_ctx* s = sub_for(c, b.w, b.h);
+    crop_in(c, s, b, true);
+    c->sub = s;
+    c->box = b;
+}
+
+// Makes the world's buffers current (the crop's state copied back) before a read of the world.
+static void box_sync(sr_ctx* c) {
+    if (c->sub) crop_out(c, c->sub, c->box);
+}
+
+static void run_steps(sr_ctx* c, uint32_t steps);
+
+static void run_box_steps(sr_ctx* c, uint32_t steps) {
+    constexpr unsigned long long kRefitEvery = 16;  // boxfit.rs REFIT_EVERY
+    sr_cost total{};
+    uint32_t done = 0;
+    while (done < steps) {
+        const unsigned long long s0 = c->box_steps;
+        // the next refit follows the step of index ≡ 0 (mod 16): after 1, 17, 33, ... steps
+        const unsigned long long next = s0 < 1 ? 1 : ((s0 - 1) / kRefitEvery + 1) * kRefitEvery + 1;
+        const uint32_t k = (uint32_t)std::min<unsigned long long>(steps - done, next - s0);
+        sr_ctx* s = c->sub;
+        run_steps(s, k);
+        if (c->timing) {
+            total.steps += s->cost.steps;
+            total.gravity_ms += s->cost.gravity_ms;
+            total.hydro_ms += s->cost.hydro_ms;
+            total.heat_ms += s->cost.heat_ms;
+            total.floors_ms += s->cost.floors_ms;
+            total.dt_ms += s->cost.dt_ms;
+            total.total_ms += s->cost.total_ms;
+            total.hydro_update_ms += s->cost.hydro_update_ms;
+            total.hydro_update_launches += s->cost.hydro_update_launches;
+            total.kernel_launches += s->cost.kernel_launches;
+        }
+        c->box_steps += k;
+        done += k;
+        if (c->box_steps == next) refit(c);
+    }
+    SR_CUDA_TRY(cudaStreamSynchronize(c->sub->stream));
+    if (c->timing) c->cost = total;
+}
+
 // Captures the whole step from the current state buffer as a graph (once per buffer).
 static void capture_step_graph(sr_ctx* c) {
     sr_ctx_prepare_capture(c);
@@ -453,6 +607,10 @@ static void capture_step_graph(sr_ctx* c) {
 }
 
 static void run_steps(sr_ctx* c, uint32_t steps) {
+    if (c->use_box) {
+        run_box_steps(c, steps);
+        return;
+    }
     const unsigned long long launches0 = sr_launches();
     // after the first step (which tunes the multigrid) every step is one captured graph, unless the per-pass timing
     // (2) asks for the passes launched one by one; timing 1 records the device time of each step's graph
@@ -611,6 +769,11 @@ sr_status sr_create(const sr_config* cfg, sr_ctx** out) {
         dalloc(&c->part_g, (size_t)fb);
         dalloc(&c->part_nf, (size_t)fb);
         if (cfg->heat) c->heat = heat_create(*cfg, c->stream);
+        c->use_box = cfg->active_box != 0;
+        if (c->use_box) {
+            dalloc(&c->box_part, 4 * (size_t)kBoxMaxBlocks);
+            dalloc(&c->box_rec, 4);
+        }
         if (c->heat && ref_mode(c)) {
             HeatRef hr;
             hr.on = 1;
@@ -648,9 +811,24 @@ sr_status sr_upload(sr_ctx* c, const float* p, uint32_t nplanes) {
             SR_CUDA_TRY(cudaMemsetAsync(c->rady, 0, sizeof(float) * c->n, c->stream));
         }
         if (c->heat) heat_reset(c->heat, c->stream);
+        c->uploaded = true;
+        if (c->use_box) {
+            // the box fit to the new state, its crop the world that steps; P2 and Δt_0 over it (boxfit.rs: before
+            // step 0, ahead of the initial Δt reduction)
+            c->sub = nullptr;
+            c->box_steps = 0;
+            const BoxRec b = fit_box(c);
+            sr_ctx* s = sub_for(c, b.w, b.h);
+            crop_in(c, s, b, false);
+            if (s->heat) heat_reset(s->heat, s->stream);
+            initial_reductions(s);
+            SR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+            c->sub = s;
+            c->box = b;
+            return;
+        }
         initial_reductions(c);
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        c->uploaded = true;
     });
 }
 
@@ -658,6 +836,7 @@ sr_status sr_readback(sr_ctx* c, float* p, uint32_t nplanes) {
     return guarded(c, [&] {
         SR_REQUIRE(p, "sr_readback: null planes");
         SR_REQUIRE((int)nplanes == c->nc, "sr_readback: the context carries " + std::to_string(c->nc) + " planes");
+        box_sync(c);
         SR_CUDA_TRY(cudaMemcpyAsync(p, planes(c), sizeof(float) * c->nc * c->n, cudaMemcpyDeviceToHost, c->stream));
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
     });
@@ -671,6 +850,12 @@ sr_status sr_upload_held(sr_ctx* c, const uint32_t* mask) {
         for (size_t i = 0; i < c->n; i++) m[i] = mask[i] != 0;
         SR_CUDA_TRY(cudaMemcpyAsync(c->held, m.data(), c->n, cudaMemcpyHostToDevice, c->stream));
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (c->sub) {
+            const BoxRec& b = c->box;
+            box_copy(c->sub->held, b.w, c->sub->n, c->held + (size_t)b.y0 * c->w + b.x0, c->w, c->n, 1, b.w, b.h, 1,
+                     c->sub->stream);
+            SR_CUDA_TRY(cudaStreamSynchronize(c->sub->stream));
+        }
     });
 }
 
@@ -678,6 +863,7 @@ sr_status sr_read_held(sr_ctx* c, uint32_t* mask) {
     return guarded(c, [&] {
         SR_REQUIRE(mask, "sr_read_held: null mask");
         SR_REQUIRE(c->held, "sr_read_held: the hold is reference mode's (a context of 14 channels)");
+        box_sync(c);
         std::vector<uint8_t> m(c->n);
         SR_CUDA_TRY(cudaMemcpyAsync(m.data(), c->held, c->n, cudaMemcpyDeviceToHost, c->stream));
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -691,11 +877,32 @@ sr_status sr_upload_opacity(sr_ctx* c, const float* kappa) {
         SR_REQUIRE(c->cfg.opacity_plane, "sr_upload_opacity: the context was made without opacity_plane");
         SR_CUDA_TRY(cudaMemcpyAsync(c->kappa, kappa, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (c->sub) {
+            const BoxRec& b = c->box;
+            box_copy(c->sub->kappa, b.w, c->sub->n, c->kappa + (size_t)b.y0 * c->w + b.x0, c->w, c->n, 1, b.w, b.h,
+                     sizeof(float), c->sub->stream);
+            SR_CUDA_TRY(cudaStreamSynchronize(c->sub->stream));
+        }
     });
 }
 
 // The checks after steps ran (the stream idle): a bounded wait that gave up, then the non-finite guard.
 static sr_status after_steps(sr_ctx* c) {
+    if (c->sub) {
+        const sr_status ss = after_steps(c->sub);
+        if (ss == SR_OK) return SR_OK;
+        c->error = c->sub->error;
+        if (ss == SR_E_NONFINITE) {  // the cell in world coordinates
+            DtRecord rec;
+            sr_status st2 = guarded(c, [&] { SR_CUDA_TRY(cudaMemcpy(&rec, c->sub->rec, sizeof rec, cudaMemcpyDeviceToHost)); });
+            if (st2 != SR_OK) return st2;
+            const BoxRec& b = c->box;
+            const long long cell = (rec.nf_cell / b.w + b.y0) * (long long)c->w + rec.nf_cell % b.w + b.x0;
+            c->error = "non-finite value at cell " + std::to_string(cell) + " channel " +
+                       std::to_string(rec.nf_channel) + " after step " + std::to_string(rec.nf_step);
+        }
+        return ss;
+    }
     sr_status st = guarded(c, [&] {
         int herr = 0;
         SR_CUDA_TRY(cudaMemcpy(&herr, c->herr, sizeof herr, cudaMemcpyDeviceToHost));
@@ -733,7 +940,14 @@ sr_status sr_read_dt(sr_ctx* c, sr_dt_report* out) {
         SR_REQUIRE(out, "sr_read_dt: null report");
         DtRecord rec;
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        SR_CUDA_TRY(cudaMemcpy(&rec, c->rec, sizeof rec, cudaMemcpyDeviceToHost));
+        if (c->sub) {
+            SR_CUDA_TRY(cudaStreamSynchronize(c->sub->stream));
+            SR_CUDA_TRY(cudaMemcpy(&rec, c->sub->rec, sizeof rec, cudaMemcpyDeviceToHost));
+            if (rec.non_finite)
+                rec.nf_cell = (rec.nf_cell / c->box.w + c->box.y0) * (long long)c->w + rec.nf_cell % c->box.w + c->box.x0;
+        } else {
+            SR_CUDA_TRY(cudaMemcpy(&rec, c->rec, sizeof rec, cudaMemcpyDeviceToHost));
+        }
         out->dt = rec.dt;
         out->dt_next = rec.dt_next;
         out->steps = rec.steps;
@@ -748,14 +962,19 @@ sr_status sr_read_heat(sr_ctx* c, sr_heat_report* out) {
     return guarded(c, [&] {
         SR_REQUIRE(out, "sr_read_heat: null report");
         SR_REQUIRE(c->cfg.heat, "sr_read_heat: the context runs no heat pass");
-        heat_report(c->heat, c->stream, &c->heat_report);
-        *out = c->heat_report;
+        sr_ctx* h = c->sub ? c->sub : c;
+        heat_report(h->heat, h->stream, &h->heat_report);
+        *out = h->heat_report;
     });
 }
 
 sr_status sr_gravity_field(sr_ctx* c, float* gx, float* gy, float* phi) {
     return guarded(c, [&] {
         SR_REQUIRE(c->cfg.gravity, "sr_gravity_field: the context runs no gravity pass");
+        if (c->sub) {  // P2 of the world's state as it stands
+            box_sync(c);
+            c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
+        }
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
         if (gx) SR_CUDA_TRY(cudaMemcpy(gx, c->gx, sizeof(float) * c->n, cudaMemcpyDeviceToHost));
         if (gy) SR_CUDA_TRY(cudaMemcpy(gy, c->gy, sizeof(float) * c->n, cudaMemcpyDeviceToHost));
@@ -767,7 +986,27 @@ sr_status sr_heat_flux(sr_ctx* c, float* fx, float* fy) {
     return guarded(c, [&] {
         SR_REQUIRE(c->cfg.heat, "sr_heat_flux: the context runs no heat pass");
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
-        heat_read_flux(c->heat, fx, fy);
+        if (!c->sub) {
+            heat_read_flux(c->heat, fx, fy);
+            return;
+        }
+        // the crop's faces at the box's place in the world's face planes; no flux crosses a face outside the box
+        sr_ctx* s = c->sub;
+        const BoxRec& b = c->box;
+        SR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+        std::vector<float> sx((size_t)(b.w + 1) * b.h), sy((size_t)b.w * (b.h + 1));
+        heat_read_flux(s->heat, sx.data(), sy.data());
+        if (fx) {
+            std::fill(fx, fx + (size_t)(c->w + 1) * c->h, 0.0f);
+            for (int y = 0; y < b.h; y++)
+                for (int x = 0; x <= b.w; x++)
+                    fx[(size_t)(y + b.y0) * (c->w + 1) + x + b.x0] = sx[(size_t)y * (b.w + 1) + x];
+        }
+        if (fy) {
+            std::fill(fy, fy + (size_t)c->w * (c->h + 1), 0.0f);
+            for (int y = 0; y <= b.h; y++)
+                for (int x = 0; x < b.w; x++) fy[(size_t)(y + b.y0) * c->w + x + b.x0] = sy[(size_t)y * b.w + x];
+        }
     });
 }
 
@@ -777,6 +1016,13 @@ sr_status sr_set_edge_mode(sr_ctx* c, uint32_t edge) {
         drop_step_graphs(c);  // the captured steps hold the edge mode
         c->cfg.edge = edge;
         c->H.edge = (int)edge;
+        c->R.edge = (int)edge;
+        for (sr_ctx* s : c->subs) {
+            drop_step_graphs(s);
+            s->cfg.edge = edge;
+            s->H.edge = (int)edge;
+            s->R.edge = (int)edge;
+        }
     });
 }
 
@@ -787,6 +1033,11 @@ sr_status sr_set_heat_precond(sr_ctx* c, uint32_t precond) {
         drop_step_graphs(c);
         c->cfg.precond = precond;
         heat_set_precond(c->heat, precond);
+        for (sr_ctx* s : c->subs) {
+            drop_step_graphs(s);
+            s->cfg.precond = precond;
+            heat_set_precond(s->heat, precond);
+        }
     });
 }
 
@@ -798,11 +1049,34 @@ sr_status sr_set_heat_limits(sr_ctx* c, uint32_t max_passes, uint32_t max_rounds
         c->cfg.max_passes = max_passes;
         c->cfg.max_rounds = max_rounds;
         heat_set_limits(c->heat, max_passes, max_rounds);
+        for (sr_ctx* s : c->subs) {
+            drop_step_graphs(s);
+            s->cfg.max_passes = max_passes;
+            s->cfg.max_rounds = max_rounds;
+            heat_set_limits(s->heat, max_passes, max_rounds);
+        }
+    });
+}
+
+sr_status sr_read_box(sr_ctx* c, sr_box_report* out) {
+    return guarded(c, [&] {
+        SR_REQUIRE(out, "sr_read_box: null report");
+        sr_ctx* g = c->sub ? c->sub : c;
+        out->x0 = c->sub ? (uint32_t)c->box.x0 : 0;
+        out->y0 = c->sub ? (uint32_t)c->box.y0 : 0;
+        out->w = (uint32_t)g->w;
+        out->h = (uint32_t)g->h;
+        out->fft_w = g->grav_ready ? (uint32_t)g->grav.px : 0;
+        out->fft_h = g->grav_ready ? (uint32_t)g->grav.py : 0;
+        out->fits = c->box_fits;
     });
 }
 
 sr_status sr_set_timing(sr_ctx* c, int32_t on) {
-    return guarded(c, [&] { c->timing = on <= 0 ? 0 : (on == 1 ? 1 : 2); });
+    return guarded(c, [&] {
+        c->timing = on <= 0 ? 0 : (on == 1 ? 1 : 2);
+        for (sr_ctx* s : c->subs) s->timing = c->timing;
+    });
 }
 
 sr_status sr_read_cost(sr_ctx* c, sr_cost* out) {
@@ -920,6 +1194,13 @@ sr_status sr_attach_learner(sr_ctx* c, sr_learner* l) {
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
         heat_attach_learned(c->heat, l ? l->L : nullptr);
         c->learner = l;
+        for (sr_ctx* s : c->subs) {
+            drop_step_graphs(s);
+            SR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+            heat_attach_learned(s->heat, l ? l->L : nullptr);
+            s->learner = l;
+            if (!l && s->cfg.precond == SR_PRECOND_LEARNED) s->cfg.precond = SR_PRECOND_MG;
+        }
         if (!l && c->cfg.precond == SR_PRECOND_LEARNED) c->cfg.precond = SR_PRECOND_MG;
     });
 }

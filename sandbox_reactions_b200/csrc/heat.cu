@@ -1682,6 +1682,8 @@ void heat_flux_planes(const HeatSolver* H, const float** fx, const float** fy) {
     *fy = H->fy;
 }
 
+double* heat_rate_plane(HeatSolver* H) { return H->rate; }
+
 void heat_set_limits(HeatSolver* H, uint32_t max_passes, uint32_t max_rounds) {
     H->max_passes = max_passes;
     H->max_rounds = max_rounds;

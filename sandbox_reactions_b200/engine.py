@@ -14,7 +14,8 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .abi import (PRECOND, EDGE, STATUS_NAMES, Config, sr_config, sr_cost, sr_dt_report, sr_heat_report)
+from .abi import (PRECOND, EDGE, STATUS_NAMES, Config, sr_box_report, sr_config, sr_cost, sr_dt_report,
+                  sr_heat_report)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsrcuda.so")
@@ -51,6 +52,7 @@ def load_library(path: str = LIB_PATH):
     L.sr_upload_opacity.argtypes = [P, F]
     L.sr_upload_held.argtypes = [P, C.POINTER(C.c_uint32)]
     L.sr_read_held.argtypes = [P, C.POINTER(C.c_uint32)]
+    L.sr_read_box.argtypes = [P, C.POINTER(sr_box_report)]
     L.sr_step.argtypes = [P, C.c_uint32]
     L.sr_read_dt.argtypes = [P, C.POINTER(sr_dt_report)]
     L.sr_read_heat.argtypes = [P, C.POINTER(sr_heat_report)]
@@ -93,7 +95,7 @@ def load_library(path: str = LIB_PATH):
         getattr(L, name).restype = C.c_int
     L.sr_last_error.restype = C.c_char_p
     L.sr_last_error.argtypes = [P]
-    for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_upload_held", "sr_read_held",
+    for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_upload_held", "sr_read_held", "sr_read_box",
                  "sr_step", "sr_read_dt",
                  "sr_read_heat", "sr_gravity_field", "sr_heat_flux", "sr_set_edge_mode", "sr_set_heat_precond",
                  "sr_set_heat_limits", "sr_set_timing", "sr_read_cost", "sr_heat_first_solve"):
@@ -176,6 +178,12 @@ class Step:
         if m.shape != self.shape[1:]:
             raise SrError(1, f"mask of shape {m.shape}, expected {self.shape[1:]}")
         self._check(self.lib.sr_upload_held(self._h, m.ctypes.data_as(C.POINTER(C.c_uint32))))
+
+    def read_box(self) -> sr_box_report:
+        """BoxFit::read (boxfit.rs:152-172): the active box's origin and size, its FFT size, the fits so far."""
+        r = sr_box_report()
+        self._check(self.lib.sr_read_box(self._h, C.byref(r)))
+        return r
 
     def read_held(self) -> np.ndarray:
         m = np.zeros(self.shape[1:], np.uint32)
