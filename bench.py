@@ -421,6 +421,45 @@ def config_runs(peak_gbs: float):
     return out
 
 
+def box_measure(n: int = 2048, steps: int = 16, warmup: int = 17):
+    """The active box (boxfit.rs) on a vacuum-heavy world: the benchmark's 2048² world (hydro + gravity + FLD) with
+    the gas past r = n/4 replaced by the floor state, stepped whole and in its box (warm-up past the first refit, then
+    `steps` steps timed on the device); the two final states compared (rel L1 per field) and each rate given in cells
+    of the whole world per second."""
+    import numpy as np
+
+    from sandbox_reactions_b200 import scenes
+    from sandbox_reactions_b200.engine import Step
+
+    cfg, P, kappa = scenes.full_step(n)
+    yy, xx = np.mgrid[0:n, 0:n]
+    out = np.hypot(xx - (n - 1) / 2.0, yy - (n - 1) / 2.0) > n / 4.0
+    P = P.copy()
+    P[0][out] = cfg.sigma_floor
+    P[1][out] = 0.0
+    P[2][out] = 0.0
+    P[3][out] = cfg.sigma_floor * cfg.t_floor / (cfg.mu * (cfg.gamma - 1.0))
+    res, states = {}, {}
+    for box in (False, True):
+        with Step(cfg.replace(active_box=box)) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            s.run(warmup)
+            s.set_timing(1)
+            s.run(steps)
+            ms = s.read_cost().total_ms
+            s.set_timing(0)
+            b = s.read_box()
+            states[box] = s.readback()
+        res["box" if box else "whole"] = {"ms_per_step": ms / steps, "value": n * n * steps / (ms / 1e3) / 1e6,
+                                          "unit": UNIT, "box": [b.x0, b.y0, b.w, b.h], "fft": [b.fft_w, b.fft_h]}
+    res["speedup"] = res["whole"]["ms_per_step"] / res["box"]["ms_per_step"]
+    res["box_vs_whole_rel_l1"] = max(rel_l1(states[True][k], states[False][k]) for k in range(4))
+    res["what"] = (f"{n}x{n} hydro+grav+FLD world, vacuum past r = {n // 4}: whole world vs the active box, "
+                   f"{warmup} warm-up steps then {steps} timed")
+    return res
+
+
 def batch_measure(count: int, steps: int, warmup: int, rank: int = 0, world: int = 1, dist=None):
     """Config 5 on this rank: its share (by cell count) of `count` worlds of a seeded 256²…2048² mix advanced as one
     batch — after the first step each batch step is one captured CUDA graph over all of them — against the same worlds
@@ -513,6 +552,7 @@ def main():
     ap.add_argument("--precond", default="mg")
     ap.add_argument("--no-fld", action="store_true", help="skip the FLD time-to-1e-8 measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-world batch (config 5) side measurement")
+    ap.add_argument("--no-box", action="store_true", help="skip the active box side measurement")
     ap.add_argument("--batch", type=int, default=0,
                     help="run config 5 instead: this many worlds of a seeded 256..2048 mix, batched vs one at a time")
     args = ap.parse_args()
@@ -627,6 +667,9 @@ def main():
     step.close()
     if rank == 0 and not args.no_batch and world == 1:
         batched = batch_measure(64, 2, 3)
+    boxed = None
+    if rank == 0 and not args.no_box and world == 1:
+        boxed = box_measure()
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -672,6 +715,7 @@ def main():
             "fld_time_to_1e-8": fld,
             "other_configs": configs,
             "batched": batched,
+            "active_box": boxed,
         }
         print(json.dumps(line), flush=True)
     if dist:
