@@ -319,6 +319,18 @@ def fld_time_to_tol(size: int):
         learner.close()
     if "ms" in out.get("learned", {}) and "ms" in out.get("mg", {}):
         out["learned_speedup_vs_mg"] = out["mg"]["ms"] / out["learned"]["ms"]
+        # why it does not pay: a learned round is two V-cycles (the second removes the BF16 output's rounding noise)
+        # plus the network; its break-even network cost from the measured MG round
+        mg_round = out["mg"]["ms"] / max(1, out["mg"]["rounds"])
+        lr = max(1, out["learned"]["rounds"])
+        out["learned_break_even"] = {
+            "mg_round_ms": mg_round,
+            "learned_round_ms": out["learned"]["ms"] / lr,
+            "network_ms_per_round": out["learned"]["ms"] / lr - 2.0 * mg_round,
+            "learned_ms_with_a_free_network": lr * 2.0 * mg_round,
+            "break_even_network_ms": (out["mg"]["ms"] - lr * 2.0 * mg_round) / lr,
+            "rounds_a_free_network_must_reach": out["mg"]["ms"] / (2.0 * mg_round),
+        }
     out.update(fld_system_checks(cfg, P, kappa, x_mg))
     return out
 

@@ -912,6 +912,8 @@ static sr_status after_steps(sr_ctx* c) {
         }
         if (c->cfg.precond == SR_PRECOND_LEARNED && c->learner && learned_error(c->learner->L, c->stream))
             throw SrError{SR_E_TIMEOUT, "a tensor-core wait of the learned preconditioner gave up"};
+        if (c->heat && heat_wait_error(c->heat, c->stream))
+            throw SrError{SR_E_TIMEOUT, "a TMA wait of the multigrid smoother gave up"};
     });
     if (st != SR_OK) return st;
     DtRecord rec;

@@ -1684,6 +1684,8 @@ void heat_flux_planes(const HeatSolver* H, const float** fx, const float** fy) {
 
 double* heat_rate_plane(HeatSolver* H) { return H->rate; }
 
+bool heat_wait_error(HeatSolver* H, cudaStream_t s) { return H->mg.error(s); }
+
 void heat_set_limits(HeatSolver* H, uint32_t max_passes, uint32_t max_rounds) {
     H->max_passes = max_passes;
     H->max_rounds = max_rounds;

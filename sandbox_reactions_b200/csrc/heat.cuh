@@ -22,6 +22,8 @@ void heat_set_reference(HeatSolver* hs, const HeatRef& R);
 void heat_flux_planes(const HeatSolver* hs, const float** fx, const float** fy);
 // Each cell's rate of the last step (W*H doubles on the device), the next step's first iterate.
 double* heat_rate_plane(HeatSolver* hs);
+// Whether a bounded device wait of the solver's multigrid gave up since the last call (clears the flag).
+bool heat_wait_error(HeatSolver* hs, cudaStream_t s);
 void heat_destroy(HeatSolver* hs);
 // One implicit step of length *dt_dev on the 4 planes U (E changes), κ from `kappa` (W*H) or cfg.kappa0.
 void heat_step(HeatSolver* hs, float* U, const float* kappa, const double* dt_dev, cudaStream_t s, sr_heat_report* rep);

@@ -7,6 +7,7 @@
 
 #include "mg.cuh"
 #include "reduce.cuh"
+#include "tma.cuh"
 
 namespace {
 
@@ -565,6 +566,196 @@ __global__ void __launch_bounds__(RB_NT, 2) mg_rowband_kernel(MgLevel L, MgLevel
     (void)SY;
 }
 
+// The row-band smoother of level 0 with its region staged by TMA: the same smoother as mg_rowband_kernel (unweighted
+// levels only), its coefficients (b, c, dx, dy) and, after the coarse correction, the iterate x read from shared memory
+// where one thread's bulk tensor copies put them — the region's 64 rows and the row above it, 72 columns from a
+// 16-byte boundary left of the region (the pair's left coupling included), zero past the level's edges — so a CTA's
+// loads are all in flight at once instead of four row-dependent rounds per thread. Every wait is bounded: a wait that
+// gives up sets the level's error flag and the CTA leaves without its stores.
+constexpr int RB_TMA_X = 72, RB_TMA_Y = RB_RY + 1;
+constexpr uint32_t kMgWaitPolls = 1u << 24;
+template <bool PRE>
+constexpr int rb_tma_arrays() { return PRE ? 4 : 5; }  // b, c, dx, dy (and x after the coarse correction)
+constexpr size_t rb_tma_array_bytes() { return ((size_t)RB_TMA_X * RB_TMA_Y * sizeof(float) + 127) / 128 * 128; }
+template <bool PRE>
+constexpr size_t rb_tma_smem() {
+    return rb_tma_arrays<PRE>() * rb_tma_array_bytes() + sizeof(float2) * 2 * 2 * RB_WARPS * 32 + 16;
+}
+
+template <int NS, bool PRE>
+__global__ void __launch_bounds__(RB_NT, 2)
+    mg_rowband_tma_kernel(const __grid_constant__ CUtensorMap mb, const __grid_constant__ CUtensorMap mc,
+                          const __grid_constant__ CUtensorMap mdx, const __grid_constant__ CUtensorMap mdy,
+                          const __grid_constant__ CUtensorMap mx, MgLevel L, MgLevel C, const float* __restrict__ xc,
+                          float omega, double* part, unsigned* counter, double* out) {
+    constexpr int H = rb_halo<NS, PRE>(), SX = RB_RX - 2 * H;
+    constexpr int XO = (H % 4 == 2) ? 2 : 4;  // the region's first column within the box (X0 - XO on a 16-byte boundary)
+    constexpr int NA = rb_tma_arrays<PRE>();
+    constexpr size_t AB = rb_tma_array_bytes() / sizeof(float);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* sarr = reinterpret_cast<float*>(smem_raw);
+    float2(*edge)[2][RB_WARPS][32] = reinterpret_cast<float2(*)[2][RB_WARPS][32]>(smem_raw + NA * rb_tma_array_bytes());
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + NA * rb_tma_array_bytes() + sizeof(float2) * 2 * 2 * RB_WARPS * 32);
+    const float* sb = sarr;
+    const float* sc = sarr + AB;
+    const float* sdx = sarr + 2 * AB;
+    const float* sdy = sarr + 3 * AB;
+    const float* sx = sarr + 4 * AB;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int w = L.w, h = L.h;
+    const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * (RB_RY - 2 * H) - H;
+    if (tid == 0) {
+        tc::mbar_init(mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (tid == 0) {
+        tma::expect_tx(mbar, (uint32_t)(NA * RB_TMA_X * RB_TMA_Y * sizeof(float)));
+        const int xs = X0 - XO, ys = Y0 - 1;
+        tma::load_3d(sarr, &mb, xs, ys, 0, mbar);
+        tma::load_3d(sarr + AB, &mc, xs, ys, 0, mbar);
+        tma::load_3d(sarr + 2 * AB, &mdx, xs, ys, 0, mbar);
+        tma::load_3d(sarr + 3 * AB, &mdy, xs, ys, 0, mbar);
+        if constexpr (!PRE) tma::load_3d(sarr + 4 * AB, &mx, xs, ys, 0, mbar);
+    }
+    const int gx = X0 + 2 * lane;
+    const bool xin = gx >= 0 && gx < w;
+    const int gy0 = Y0 + RB_R * warp;
+    // the coarse correction of the post-smoother (global, half resolution) is read while the boxes land
+    float corr[RB_R];
+#pragma unroll
+    for (int r = 0; r < RB_R; r++) {
+        const int gy = gy0 + r;
+        corr[r] = (!PRE && xin && gy >= 0 && gy < h) ? omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)] : 0.0f;
+    }
+    const bool landed = tc::mbar_wait(mbar, 0, kMgWaitPolls);
+    if (__syncthreads_or(!landed)) {
+        if (tid == 0 && L.err) atomicOr(L.err, 1);
+        tc::mbar_wait(mbar, 0, kMgWaitPolls);  // copies still in flight land before the CTA leaves
+        return;
+    }
+    float bA[RB_R], bB[RB_R], iA[RB_R], iB[RB_R], dl[RB_R], dm[RB_R], dr[RB_R], dA[RB_R], dB[RB_R];
+    float xA[RB_R], xB[RB_R], cA[RB_R], cB[RB_R];
+    float uA = 0.0f, uB = 0.0f;
+    const int col0 = XO + 2 * lane;  // the pair's first column within the box
+#pragma unroll
+    for (int r = 0; r < RB_R; r++) {
+        const int gy = gy0 + r;
+        const bool in = xin && gy >= 0 && gy < h;
+        const int q = (RB_R * warp + r + 1) * RB_TMA_X + col0;  // the box's row 0 is the region's row -1
+        float2 b2 = make_float2(0.f, 0.f), c2 = make_float2(1.f, 1.f), dx2 = b2, dy2 = b2;
+        float left = 0.0f;
+        if (in) {
+            b2 = *reinterpret_cast<const float2*>(sb + q);
+            c2 = *reinterpret_cast<const float2*>(sc + q);
+            dx2 = *reinterpret_cast<const float2*>(sdx + q);
+            dy2 = *reinterpret_cast<const float2*>(sdy + q);
+            left = sdx[q - 1];  // zero past the level's left edge
+            if (r == 0) {
+                const float2 u2 = *reinterpret_cast<const float2*>(sdy + q - RB_TMA_X);  // zero above row 0
+                uA = u2.x;
+                uB = u2.y;
+            }
+        }
+        bA[r] = b2.x;
+        bB[r] = b2.y;
+        cA[r] = c2.x;
+        cB[r] = c2.y;
+        dm[r] = dx2.x;
+        dr[r] = dx2.y;
+        dA[r] = dy2.x;
+        dB[r] = dy2.y;
+        dl[r] = left;
+        const float upA = r ? dA[r - 1] : uA, upB = r ? dB[r - 1] : uB;
+        iA[r] = in ? __fdividef(1.0f, c2.x + dl[r] + dx2.x + upA + dy2.x) : 0.0f;
+        iB[r] = in ? __fdividef(1.0f, c2.y + dx2.x + dx2.y + upB + dy2.y) : 0.0f;
+        float x0 = 0.0f, x1 = 0.0f;
+        if (!PRE && in) {
+            const float2 xv = *reinterpret_cast<const float2*>(sx + q);
+            x0 = xv.x + corr[r];
+            x1 = xv.y + corr[r];
+        }
+        xA[r] = x0;
+        xB[r] = x1;
+    }
+    edge[0][0][warp][lane] = make_float2(xA[0], xB[0]);
+    edge[0][1][warp][lane] = make_float2(xA[RB_R - 1], xB[RB_R - 1]);
+    __syncthreads();
+    const int wu = warp > 0 ? warp - 1 : warp, wd = warp + 1 < RB_WARPS ? warp + 1 : warp;
+#pragma unroll
+    for (int s = 0; s < NS; s++) {
+        const int col = PRE ? (s & 1) : 1 - (s & 1);
+        const int rd = s & 1, wr = (s + 1) & 1;
+        const float2 above = edge[rd][1][wu][lane], below = edge[rd][0][wd][lane];
+#pragma unroll
+        for (int r = 0; r < RB_R; r++) {
+            if ((r & 1) == col) {
+                const float left = __shfl_up_sync(0xffffffffu, xB[r], 1);
+                const float up = r ? xA[r - 1] : above.x, down = r + 1 < RB_R ? xA[r + 1] : below.x;
+                const float cu = r ? dA[r - 1] : uA;
+                xA[r] = (bA[r] + dl[r] * left + dm[r] * xB[r] + cu * up + dA[r] * down) * iA[r];
+            } else {
+                const float right = __shfl_down_sync(0xffffffffu, xA[r], 1);
+                const float up = r ? xB[r - 1] : above.y, down = r + 1 < RB_R ? xB[r + 1] : below.y;
+                const float cu = r ? dB[r - 1] : uB;
+                xB[r] = (bB[r] + dm[r] * xA[r] + dr[r] * right + cu * up + dB[r] * down) * iB[r];
+            }
+        }
+        edge[wr][0][warp][lane] = make_float2(xA[0], xB[0]);
+        edge[wr][1][warp][lane] = make_float2(xA[RB_R - 1], xB[RB_R - 1]);
+        __syncthreads();
+    }
+    const bool xout = xin && 2 * lane >= H && 2 * lane < RB_RX - H;
+    if constexpr (PRE) {
+        const float2 above = edge[NS & 1][1][wu][lane], below = edge[NS & 1][0][wd][lane];
+        float ragg[RB_R / 2] = {};
+#pragma unroll
+        for (int r = 0; r < RB_R; r++) {
+            const int gy = gy0 + r, ly = RB_R * warp + r;
+            const bool o = xout && ly >= H && ly < RB_RY - H && gy < h;
+            const size_t i = (size_t)gy * w + gx;
+            if (o) *reinterpret_cast<float2*>(L.x + i) = make_float2(xA[r], xB[r]);
+            const float left = __shfl_up_sync(0xffffffffu, xB[r], 1);
+            const float right = __shfl_down_sync(0xffffffffu, xA[r], 1);
+            const float upA = r ? xA[r - 1] : above.x, dnA = r + 1 < RB_R ? xA[r + 1] : below.x;
+            const float upB = r ? xB[r - 1] : above.y, dnB = r + 1 < RB_R ? xB[r + 1] : below.y;
+            const float cuA = r ? dA[r - 1] : uA, cuB = r ? dB[r - 1] : uB;
+            float axA = cA[r] * xA[r];
+            axA += dl[r] * (xA[r] - left);
+            axA += dm[r] * (xA[r] - xB[r]);
+            axA += cuA * (xA[r] - upA);
+            axA += dA[r] * (xA[r] - dnA);
+            float axB = cB[r] * xB[r];
+            axB += dm[r] * (xB[r] - xA[r]);
+            axB += dr[r] * (xB[r] - right);
+            axB += cuB * (xB[r] - upB);
+            axB += dB[r] * (xB[r] - dnB);
+            ragg[r >> 1] += (bA[r] - axA) + (bB[r] - axB);
+        }
+#pragma unroll
+        for (int k = 0; k < RB_R / 2; k++) {
+            const int ly = RB_R * warp + 2 * k;
+            const int X = gx >> 1, Y = (gy0 + 2 * k) >> 1;
+            if (xout && ly >= H && ly < RB_RY - H && X < C.w && Y < C.h && gy0 + 2 * k >= 0) {
+                const size_t I = (size_t)Y * C.w + X;
+                C.b[I] = C.mask[I] ? ragg[k] : 0.0f;
+            }
+        }
+    } else {
+        double acc = 0.0;
+#pragma unroll
+        for (int r = 0; r < RB_R; r++) {
+            const int gy = gy0 + r, ly = RB_R * warp + r;
+            if (xout && ly >= H && ly < RB_RY - H && gy < h) {
+                const size_t i = (size_t)gy * w + gx;
+                *reinterpret_cast<float2*>(L.x2 + i) = make_float2(xA[r], xB[r]);
+                if (out) acc += (double)bA[r] * (double)xA[r] + (double)bB[r] * (double)xB[r];
+            }
+        }
+        if (out) grid_sum_last1(acc, part, counter, out);
+    }
+}
+
 // The coarsest level's operator inverted by Gauss-Jordan elimination in f64 in one CTA (n <= 64 cells), masked-out
 // cells as identity rows; stored f32. The operator is SPD, so no pivoting is needed. The augmented matrix [A | I] is
 // kept twice and each elimination step reads one copy and writes the other, so a step is one pass and one barrier;
@@ -953,6 +1144,28 @@ void launch_rowband(const MgLevel& L, const MgLevel& C, const float* xc, float o
                     double* out, cudaStream_t s) {
     constexpr int H = rb_halo<NS, PRE>();
     const dim3 grid(div_up(L.w, RB_RX - 2 * H), div_up(L.h, RB_RY - 2 * H));
+    // level 0 (unweighted, rows of 16 bytes and 16-byte bases): the region staged by TMA
+    auto aligned = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+    if (!L.t && L.w % 4 == 0 && aligned(L.b) && aligned(L.c) && aligned(L.dx) && aligned(L.dy) &&
+        (PRE || aligned(L.x))) {
+        static bool attr = false;  // this instance's shared-memory attribute, once per process
+        if (!attr) {
+            SR_CUDA_TRY(cudaFuncSetAttribute(mg_rowband_tma_kernel<NS, PRE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rb_tma_smem<PRE>()));
+            attr = true;
+        }
+        CUtensorMap mb, mc, mdx, mdy, mx;
+        tma_encode_planes(&mb, L.b, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
+        tma_encode_planes(&mc, L.c, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
+        tma_encode_planes(&mdx, L.dx, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
+        tma_encode_planes(&mdy, L.dy, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
+        if (PRE) mx = mb;
+        else tma_encode_planes(&mx, L.x, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
+        mg_rowband_tma_kernel<NS, PRE><<<grid, RB_NT, rb_tma_smem<PRE>(), s>>>(mb, mc, mdx, mdy, mx, L, C, xc, omega,
+                                                                              part, counter, out);
+        sr_note_launch();
+        return;
+    }
     if (L.t) mg_rowband_kernel<NS, PRE, true><<<grid, RB_NT, 0, s>>>(L, C, xc, omega, part, counter, out);
     else mg_rowband_kernel<NS, PRE, false><<<grid, RB_NT, 0, s>>>(L, C, xc, omega, part, counter, out);
     sr_note_launch();
@@ -1060,6 +1273,9 @@ void Multigrid::create(int w, int h, int pre_, int post_) {
     SR_REQUIRE(nc <= 64, "the coarsest level holds more than 64 cells");
     SR_CUDA_TRY(cudaMalloc(&coarse_inv, sizeof(float) * nc * nc));
     SR_CUDA_TRY(cudaMalloc(&tail_img, ts));
+    SR_CUDA_TRY(cudaMalloc(&err, sizeof(int)));
+    SR_CUDA_TRY(cudaMemset(err, 0, sizeof(int)));
+    for (int l = 0; l < nlevels; l++) L[l].err = err;
     SR_CUDA_TRY(cudaFuncSetAttribute(mg_coarse_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(2 * nc * 2 * nc * sizeof(double))));
     set_attributes_ns<2>();
@@ -1085,7 +1301,18 @@ void Multigrid::destroy() {
     coarse_inv = nullptr;
     cudaFree(tail_img);
     tail_img = nullptr;
+    cudaFree(err);
+    err = nullptr;
     nlevels = 0;
+}
+
+bool Multigrid::error(cudaStream_t s) {
+    if (!err) return false;
+    int v = 0;
+    SR_CUDA_TRY(cudaMemcpyAsync(&v, err, sizeof v, cudaMemcpyDeviceToHost, s));
+    SR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (v) SR_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
+    return v != 0;
 }
 
 size_t Multigrid::bytes() const {

@@ -30,6 +30,7 @@ struct MgLevel {
     float* x = nullptr;   // the pre-smoother's iterate
     float* x2 = nullptr;  // the post-smoother's result (a second buffer: neighbouring tiles read x's halo meanwhile)
     float* t = nullptr;   // the cell's weight in its aggregate's basis function (null: 1, level 0)
+    int* err = nullptr;   // set to 1 when a bounded wait of a smoother gave up (its TMA boxes never landed)
 };
 
 // At most this many CTAs in one smoother launch on a w x h level (each writes one grid-sum partial at level 0).
@@ -44,6 +45,7 @@ struct Multigrid {
     float* coarse_inv = nullptr;  // the coarsest level's operator inverted (at most 64 x 64), per Newton pass
     float* tail_img = nullptr;    // the coarse tail's shared-memory image (coefficients, inverse diagonals, weights,
                                   // masks, the coarsest inverse), packed once per Newton pass
+    int* err = nullptr;           // the smoothers' error flag (MgLevel::err of every level)
 
     void create(int w, int h, int pre, int post);
     void destroy();
@@ -61,4 +63,6 @@ struct Multigrid {
     // The device time (ms) of one launch of level 0's pre- and post-smoother on the last applied system, each
     // averaged over `reps` launches with `flush` (flush_bytes, larger than L2) rewritten before each: a timing hook.
     void time_level0(int reps, void* flush, size_t flush_bytes, cudaStream_t s, double* pre_ms, double* post_ms);
+    // Whether a smoother's bounded wait gave up since the last call (reads and clears the flag; waits for `s`).
+    bool error(cudaStream_t s);
 };
