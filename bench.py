@@ -691,7 +691,7 @@ def main():
         sm_ms = pre_ms + post_ms
         achieved = sm_bytes / (sm_ms / 1e3) / 1e9 if sm_ms > 0 else None
         tr_pre, tr_post = committed_traffic("mg_smooth_pre_level0", n * n), committed_traffic("mg_smooth_post_level0", n * n)
-        roofline = {"kernel": "mg_rowband_kernel level 0 (pre + post, one V-cycle)", "bound": "hbm",
+        roofline = {"kernel": "mg_rowband_tma_kernel level 0 (pre + post, one V-cycle)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                     "frac": achieved / peak if achieved else None,
                     "traffic": (tr_pre + tr_post) if tr_pre and tr_post else None,

@@ -621,12 +621,19 @@ __global__ void __launch_bounds__(RB_NT, 2)
     const int gx = X0 + 2 * lane;
     const bool xin = gx >= 0 && gx < w;
     const int gy0 = Y0 + RB_R * warp;
-    // the coarse correction of the post-smoother (global, half resolution) is read while the boxes land
+    // read while the boxes land: the post-smoother's coarse correction, the pre-smoother's coarse mask (global, half
+    // resolution)
     float corr[RB_R];
+    uint8_t cmask[RB_R / 2];
 #pragma unroll
     for (int r = 0; r < RB_R; r++) {
         const int gy = gy0 + r;
         corr[r] = (!PRE && xin && gy >= 0 && gy < h) ? omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)] : 0.0f;
+    }
+#pragma unroll
+    for (int k = 0; k < RB_R / 2; k++) {
+        const int X = gx >> 1, Y = (gy0 + 2 * k) >> 1;
+        cmask[k] = (PRE && xin && gy0 + 2 * k >= 0 && X < C.w && Y < C.h) ? C.mask[(size_t)Y * C.w + X] : 0;
     }
     const bool landed = tc::mbar_wait(mbar, 0, kMgWaitPolls);
     if (__syncthreads_or(!landed)) {
@@ -689,6 +696,11 @@ __global__ void __launch_bounds__(RB_NT, 2)
         const float2 above = edge[rd][1][wu][lane], below = edge[rd][0][wd][lane];
 #pragma unroll
         for (int r = 0; r < RB_R; r++) {
+            if (PRE && s == 0) {  // the pre-smoother starts from x = 0: its first half-sweep is b times the inverse
+                if ((r & 1) == col) xA[r] = bA[r] * iA[r];
+                else xB[r] = bB[r] * iB[r];
+                continue;
+            }
             if ((r & 1) == col) {
                 const float left = __shfl_up_sync(0xffffffffu, xB[r], 1);
                 const float up = r ? xA[r - 1] : above.x, down = r + 1 < RB_R ? xA[r + 1] : below.x;
@@ -736,10 +748,8 @@ __global__ void __launch_bounds__(RB_NT, 2)
         for (int k = 0; k < RB_R / 2; k++) {
             const int ly = RB_R * warp + 2 * k;
             const int X = gx >> 1, Y = (gy0 + 2 * k) >> 1;
-            if (xout && ly >= H && ly < RB_RY - H && X < C.w && Y < C.h && gy0 + 2 * k >= 0) {
-                const size_t I = (size_t)Y * C.w + X;
-                C.b[I] = C.mask[I] ? ragg[k] : 0.0f;
-            }
+            if (xout && ly >= H && ly < RB_RY - H && X < C.w && Y < C.h && gy0 + 2 * k >= 0)
+                C.b[(size_t)Y * C.w + X] = cmask[k] ? ragg[k] : 0.0f;
         }
     } else {
         double acc = 0.0;
