@@ -435,9 +435,10 @@ def config_runs(peak_gbs: float):
 
 def box_measure(n: int = 2048, steps: int = 16, warmup: int = 17):
     """The active box (boxfit.rs) on a vacuum-heavy world: the benchmark's 2048² world (hydro + gravity + FLD) with
-    the gas past r = n/4 replaced by the floor state, stepped whole and in its box (warm-up past the first refit, then
-    `steps` steps timed on the device); the two final states compared (rel L1 per field) and each rate given in cells
-    of the whole world per second."""
+    the gas past r = 480 cells replaced by the floor state (a box of 976², whose FFT pads to 2048² where the world's
+    pads to 4096²), stepped whole and in its box (warm-up past the first refit, then `steps` steps timed on the
+    device); the two final states compared (rel L1 per field) and each rate given in cells of the whole world per
+    second."""
     import numpy as np
 
     from sandbox_reactions_b200 import scenes
@@ -445,7 +446,8 @@ def box_measure(n: int = 2048, steps: int = 16, warmup: int = 17):
 
     cfg, P, kappa = scenes.full_step(n)
     yy, xx = np.mgrid[0:n, 0:n]
-    out = np.hypot(xx - (n - 1) / 2.0, yy - (n - 1) / 2.0) > n / 4.0
+    radius = 480.0 * n / 2048.0
+    out = np.hypot(xx - (n - 1) / 2.0, yy - (n - 1) / 2.0) > radius
     P = P.copy()
     P[0][out] = cfg.sigma_floor
     P[1][out] = 0.0
@@ -467,7 +469,7 @@ def box_measure(n: int = 2048, steps: int = 16, warmup: int = 17):
                                           "unit": UNIT, "box": [b.x0, b.y0, b.w, b.h], "fft": [b.fft_w, b.fft_h]}
     res["speedup"] = res["whole"]["ms_per_step"] / res["box"]["ms_per_step"]
     res["box_vs_whole_rel_l1"] = max(rel_l1(states[True][k], states[False][k]) for k in range(4))
-    res["what"] = (f"{n}x{n} hydro+grav+FLD world, vacuum past r = {n // 4}: whole world vs the active box, "
+    res["what"] = (f"{n}x{n} hydro+grav+FLD world, vacuum past r = {radius:.0f}: whole world vs the active box, "
                    f"{warmup} warm-up steps then {steps} timed")
     return res
 
