@@ -35,6 +35,14 @@ __device__ __constant__ float kSin16[16] = {0.0f, 3.826834324e-01f, 7.071067812e
                                              -3.826834324e-01f, -7.071067812e-01f, -9.238795325e-01f, -1.0f,
                                              -9.238795325e-01f, -7.071067812e-01f, -3.826834324e-01f};
 
+// Shared-memory FFT buffers hold one float2 of padding after every 16 points: the radix-16 stages' scattered writes
+// (stride Ns·16 elements in the first stage) and strided reads then fall on different banks.
+__device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
+template <int N>
+constexpr int fft_len() {
+    return N + N / 16;
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
@@ -81,7 +89,7 @@ __device__ __forceinline__ void stockham_stage(float2* buf, const float2* __rest
             const int j = t + b * (N / 16);
             const int k = j % Ns;
 #pragma unroll
-            for (int r = 0; r < R; r++) v[b][r] = buf[j + r * (N / R)];
+            for (int r = 0; r < R; r++) v[b][r] = buf[fpad(j + r * (N / R))];
             if (Ns > 1) {
                 const int step = N / (Ns * R);
 #pragma unroll
@@ -102,7 +110,7 @@ __device__ __forceinline__ void stockham_stage(float2* buf, const float2* __rest
             const int k = j % Ns;
             const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
-            for (int r = 0; r < R; r++) buf[base + r * Ns] = v[b][r];
+            for (int r = 0; r < R; r++) buf[fpad(base + r * Ns)] = v[b][r];
         }
     }
     __syncthreads();
@@ -145,7 +153,7 @@ __global__ void __launch_bounds__(2 * fft_threads<N>()) grav_rows_kernel(GravArg
     extern __shared__ float2 sm[];
     constexpr int T = fft_threads<N>();
     const int f = threadIdx.x / T, t = threadIdx.x % T;
-    float2* buf = sm + f * N;
+    float2* buf = sm + f * fft_len<N>();
     const int ya = blockIdx.x * 4 + 2 * f, yb = ya + 1;
     const int w = A.w, h = A.h;
     const float sv = A.sigma_vac;
@@ -161,14 +169,14 @@ __global__ void __launch_bounds__(2 * fft_threads<N>()) grav_rows_kernel(GravArg
                 b = s >= sv ? s : 0.0f;
             }
         }
-        buf[x] = make_float2(a, b);
+        buf[fpad(x)] = make_float2(a, b);
     }
     __syncthreads();
     fft_smem<N, false>(buf, A.tw_x, t, t < N / 16);
     // unpack: X_a[k] = (Z[k] + conj Z[N-k]) / 2, X_b[k] = (Z[k] - conj Z[N-k]) / 2i, k = 0..N/2; column-major out
     const size_t ld = A.ld;
     for (int k = t; k <= N / 2; k += T) {
-        float2 z = buf[k], zc = buf[(N - k) & (N - 1)];
+        float2 z = buf[fpad(k)], zc = buf[fpad((N - k) & (N - 1))];
         float2 xa = make_float2(0.5f * (z.x + zc.x), 0.5f * (z.y - zc.y));
         float2 xb = make_float2(0.5f * (z.y + zc.y), 0.5f * (zc.x - z.x));
         if (ya < h) A.spec[(size_t)k * ld + 1 + ya] = xa;
@@ -186,18 +194,18 @@ __global__ void __launch_bounds__(fft_threads<N>()) grav_columns_kernel(GravArgs
     const int h = A.h;
     const size_t ld = A.ld;
     float2* col = A.spec + (size_t)kx * ld;
-    for (int y = t; y < N; y += T) sm[y] = y < h ? col[1 + y] : make_float2(0.0f, 0.0f);
+    for (int y = t; y < N; y += T) sm[fpad(y)] = y < h ? col[1 + y] : make_float2(0.0f, 0.0f);
     __syncthreads();
     fft_smem<N, false>(sm, A.tw_y, t, t < N / 16);
     const float* kq = A.khat + (size_t)kx * (N / 2 + 1);
     for (int ky = t; ky < N; ky += T) {
         float k = kq[ky <= N / 2 ? ky : N - ky];
-        float2 z = sm[ky];
-        sm[ky] = make_float2(z.x * k, z.y * k);
+        float2 z = sm[fpad(ky)];
+        sm[fpad(ky)] = make_float2(z.x * k, z.y * k);
     }
     __syncthreads();
     fft_smem<N, true>(sm, A.tw_y, t, t < N / 16);
-    for (int r = t; r < h + 2; r += T) col[r] = sm[(r - 1 + N) & (N - 1)];
+    for (int r = t; r < h + 2; r += T) col[r] = sm[fpad((r - 1 + N) & (N - 1))];
 }
 
 // ---- pass 3: two output rows per complex inverse FFT, two FFTs per CTA; columns -1..w kept into φ_ring
@@ -206,7 +214,7 @@ __global__ void __launch_bounds__(2 * fft_threads<N>()) grav_rows_inverse_kernel
     extern __shared__ float2 sm[];
     constexpr int T = fft_threads<N>();
     const int f = threadIdx.x / T, t = threadIdx.x % T;
-    float2* buf = sm + f * N;
+    float2* buf = sm + f * fft_len<N>();
     const int rows = A.h + 2;
     const int ra = blockIdx.x * 4 + 2 * f, rb = ra + 1;
     const size_t ld = A.ld;
@@ -214,14 +222,14 @@ __global__ void __launch_bounds__(2 * fft_threads<N>()) grav_rows_inverse_kernel
         float2 xa = ra < rows ? A.spec[(size_t)k * ld + ra] : make_float2(0.0f, 0.0f);
         float2 xb = rb < rows ? A.spec[(size_t)k * ld + rb] : make_float2(0.0f, 0.0f);
         // Z[k] = X_a[k] + i X_b[k]; Z[N-k] = conj X_a[k] + i conj X_b[k]
-        buf[k] = make_float2(xa.x - xb.y, xa.y + xb.x);
-        if (k > 0 && k < N / 2) buf[N - k] = make_float2(xa.x + xb.y, xb.x - xa.y);
+        buf[fpad(k)] = make_float2(xa.x - xb.y, xa.y + xb.x);
+        if (k > 0 && k < N / 2) buf[fpad(N - k)] = make_float2(xa.x + xb.y, xb.x - xa.y);
     }
     __syncthreads();
     fft_smem<N, true>(buf, A.tw_x, t, t < N / 16);
     const int w = A.w, rw = w + 2;
     for (int c = t; c < rw; c += T) {
-        float2 z = buf[(c - 1 + N) & (N - 1)];
+        float2 z = buf[fpad((c - 1 + N) & (N - 1))];
         if (ra < rows) A.phi_ring[(size_t)ra * rw + c] = z.x;
         if (rb < rows) A.phi_ring[(size_t)rb * rw + c] = z.y;
     }
@@ -244,7 +252,7 @@ __global__ void grav_gradient_kernel(GravArgs A) {
 
 template <int N>
 void launch_rows(const GravArgs& A, cudaStream_t s) {
-    size_t smem = 2 * N * sizeof(float2);
+    size_t smem = 2 * fft_len<N>() * sizeof(float2);
     cudaFuncSetAttribute(grav_rows_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     grav_rows_kernel<N><<<div_up(A.h, 4), 2 * fft_threads<N>(), smem, s>>>(A);
     sr_note_launch();
@@ -252,7 +260,7 @@ void launch_rows(const GravArgs& A, cudaStream_t s) {
 
 template <int N>
 void launch_columns(const GravArgs& A, cudaStream_t s) {
-    size_t smem = N * sizeof(float2);
+    size_t smem = fft_len<N>() * sizeof(float2);
     cudaFuncSetAttribute(grav_columns_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     grav_columns_kernel<N><<<A.px / 2 + 1, fft_threads<N>(), smem, s>>>(A);
     sr_note_launch();
@@ -260,7 +268,7 @@ void launch_columns(const GravArgs& A, cudaStream_t s) {
 
 template <int N>
 void launch_rows_inverse(const GravArgs& A, cudaStream_t s) {
-    size_t smem = 2 * N * sizeof(float2);
+    size_t smem = 2 * fft_len<N>() * sizeof(float2);
     cudaFuncSetAttribute(grav_rows_inverse_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     grav_rows_inverse_kernel<N><<<div_up(A.h + 2, 4), 2 * fft_threads<N>(), smem, s>>>(A);
     sr_note_launch();
