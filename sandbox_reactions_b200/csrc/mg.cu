@@ -574,15 +574,17 @@ __global__ void __launch_bounds__(RB_NT, 2) mg_rowband_kernel(MgLevel L, MgLevel
 // gives up sets the level's error flag and the CTA leaves without its stores.
 constexpr int RB_TMA_X = 72, RB_TMA_Y = RB_RY + 1;
 constexpr uint32_t kMgWaitPolls = 1u << 24;
-template <bool PRE>
-constexpr int rb_tma_arrays() { return PRE ? 4 : 5; }  // b, c, dx, dy (and x after the coarse correction)
+// b, c, dx, dy, then x after the coarse correction (post) or the weights the restriction takes (pre, weighted levels);
+// the post-smoother of a weighted level reads its weights while the boxes land
+template <bool PRE, bool WT>
+constexpr int rb_tma_arrays() { return PRE ? (WT ? 5 : 4) : 5; }
 constexpr size_t rb_tma_array_bytes() { return ((size_t)RB_TMA_X * RB_TMA_Y * sizeof(float) + 127) / 128 * 128; }
-template <bool PRE>
+template <bool PRE, bool WT>
 constexpr size_t rb_tma_smem() {
-    return rb_tma_arrays<PRE>() * rb_tma_array_bytes() + sizeof(float2) * 2 * 2 * RB_WARPS * 32 + 16;
+    return rb_tma_arrays<PRE, WT>() * rb_tma_array_bytes() + sizeof(float2) * 2 * 2 * RB_WARPS * 32 + 16;
 }
 
-template <int NS, bool PRE>
+template <int NS, bool PRE, bool WT>
 __global__ void __launch_bounds__(RB_NT, 2)
     mg_rowband_tma_kernel(const __grid_constant__ CUtensorMap mb, const __grid_constant__ CUtensorMap mc,
                           const __grid_constant__ CUtensorMap mdx, const __grid_constant__ CUtensorMap mdy,
@@ -590,7 +592,7 @@ __global__ void __launch_bounds__(RB_NT, 2)
                           float omega, double* part, unsigned* counter, double* out) {
     constexpr int H = rb_halo<NS, PRE>(), SX = RB_RX - 2 * H;
     constexpr int XO = (H % 4 == 2) ? 2 : 4;  // the region's first column within the box (X0 - XO on a 16-byte boundary)
-    constexpr int NA = rb_tma_arrays<PRE>();
+    constexpr int NA = rb_tma_arrays<PRE, WT>();
     constexpr size_t AB = rb_tma_array_bytes() / sizeof(float);
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* sarr = reinterpret_cast<float*>(smem_raw);
@@ -600,7 +602,7 @@ __global__ void __launch_bounds__(RB_NT, 2)
     const float* sc = sarr + AB;
     const float* sdx = sarr + 2 * AB;
     const float* sdy = sarr + 3 * AB;
-    const float* sx = sarr + 4 * AB;
+    const float* sx = sarr + 4 * AB;  // post: the iterate; pre of a weighted level: the weights
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int w = L.w, h = L.h;
     const int X0 = blockIdx.x * SX - H, Y0 = blockIdx.y * (RB_RY - 2 * H) - H;
@@ -616,19 +618,29 @@ __global__ void __launch_bounds__(RB_NT, 2)
         tma::load_3d(sarr + AB, &mc, xs, ys, 0, mbar);
         tma::load_3d(sarr + 2 * AB, &mdx, xs, ys, 0, mbar);
         tma::load_3d(sarr + 3 * AB, &mdy, xs, ys, 0, mbar);
-        if constexpr (!PRE) tma::load_3d(sarr + 4 * AB, &mx, xs, ys, 0, mbar);
+        if constexpr (NA == 5) tma::load_3d(sarr + 4 * AB, &mx, xs, ys, 0, mbar);
     }
     const int gx = X0 + 2 * lane;
     const bool xin = gx >= 0 && gx < w;
     const int gy0 = Y0 + RB_R * warp;
     // read while the boxes land: the post-smoother's coarse correction, the pre-smoother's coarse mask (global, half
     // resolution)
-    float corr[RB_R];
+    float corrA[RB_R], corrB[RB_R];
     uint8_t cmask[RB_R / 2];
 #pragma unroll
     for (int r = 0; r < RB_R; r++) {
         const int gy = gy0 + r;
-        corr[r] = (!PRE && xin && gy >= 0 && gy < h) ? omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)] : 0.0f;
+        const bool in = !PRE && xin && gy >= 0 && gy < h;
+        const float cr = in ? omega * xc[(size_t)(gy >> 1) * C.w + (gx >> 1)] : 0.0f;
+        corrA[r] = cr;
+        corrB[r] = cr;
+        if constexpr (WT && !PRE) {  // the prolongation's weights
+            if (in) {
+                const float2 t2 = *reinterpret_cast<const float2*>(L.t + (size_t)gy * w + gx);
+                corrA[r] = cr * t2.x;
+                corrB[r] = cr * t2.y;
+            }
+        }
     }
 #pragma unroll
     for (int k = 0; k < RB_R / 2; k++) {
@@ -679,8 +691,8 @@ __global__ void __launch_bounds__(RB_NT, 2)
         float x0 = 0.0f, x1 = 0.0f;
         if (!PRE && in) {
             const float2 xv = *reinterpret_cast<const float2*>(sx + q);
-            x0 = xv.x + corr[r];
-            x1 = xv.y + corr[r];
+            x0 = xv.x + corrA[r];
+            x1 = xv.y + corrB[r];
         }
         xA[r] = x0;
         xB[r] = x1;
@@ -742,7 +754,13 @@ __global__ void __launch_bounds__(RB_NT, 2)
             axB += dr[r] * (xB[r] - right);
             axB += cuB * (xB[r] - upB);
             axB += dB[r] * (xB[r] - dnB);
-            ragg[r >> 1] += (bA[r] - axA) + (bB[r] - axB);
+            float rA = bA[r] - axA, rB = bB[r] - axB;
+            if constexpr (WT) {  // the restriction's weights, zero past the level (the box's fill)
+                const float2 t2 = *reinterpret_cast<const float2*>(sx + (RB_R * warp + r + 1) * RB_TMA_X + col0);
+                rA *= t2.x;
+                rB *= t2.y;
+            }
+            ragg[r >> 1] += rA + rB;
         }
 #pragma unroll
         for (int k = 0; k < RB_R / 2; k++) {
@@ -1154,25 +1172,28 @@ void launch_rowband(const MgLevel& L, const MgLevel& C, const float* xc, float o
                     double* out, cudaStream_t s) {
     constexpr int H = rb_halo<NS, PRE>();
     const dim3 grid(div_up(L.w, RB_RX - 2 * H), div_up(L.h, RB_RY - 2 * H));
-    // level 0 (unweighted, rows of 16 bytes and 16-byte bases): the region staged by TMA
+    // rows of 16 bytes and 16-byte bases: the region staged by TMA
     auto aligned = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
-    if (!L.t && L.w % 4 == 0 && aligned(L.b) && aligned(L.c) && aligned(L.dx) && aligned(L.dy) &&
-        (PRE || aligned(L.x))) {
-        static bool attr = false;  // this instance's shared-memory attribute, once per process
-        if (!attr) {
-            SR_CUDA_TRY(cudaFuncSetAttribute(mg_rowband_tma_kernel<NS, PRE>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rb_tma_smem<PRE>()));
-            attr = true;
-        }
+    if (L.w % 4 == 0 && aligned(L.b) && aligned(L.c) && aligned(L.dx) && aligned(L.dy) && aligned(L.x) &&
+        (!L.t || aligned(L.t))) {
         CUtensorMap mb, mc, mdx, mdy, mx;
         tma_encode_planes(&mb, L.b, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
         tma_encode_planes(&mc, L.c, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
         tma_encode_planes(&mdx, L.dx, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
         tma_encode_planes(&mdy, L.dy, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
-        if (PRE) mx = mb;
-        else tma_encode_planes(&mx, L.x, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
-        mg_rowband_tma_kernel<NS, PRE><<<grid, RB_NT, rb_tma_smem<PRE>(), s>>>(mb, mc, mdx, mdy, mx, L, C, xc, omega,
-                                                                              part, counter, out);
+        if (!PRE) tma_encode_planes(&mx, L.x, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
+        else if (L.t) tma_encode_planes(&mx, L.t, L.w, L.h, 1, RB_TMA_X, RB_TMA_Y);
+        else mx = mb;
+        auto go = [&](auto kernel, size_t smem, bool& attr) {
+            if (!attr) {  // the instance's shared-memory attribute, once per process
+                SR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                attr = true;
+            }
+            kernel<<<grid, RB_NT, smem, s>>>(mb, mc, mdx, mdy, mx, L, C, xc, omega, part, counter, out);
+        };
+        static bool attr_w = false, attr_u = false;
+        if (L.t) go(mg_rowband_tma_kernel<NS, PRE, true>, rb_tma_smem<PRE, true>(), attr_w);
+        else go(mg_rowband_tma_kernel<NS, PRE, false>, rb_tma_smem<PRE, false>(), attr_u);
         sr_note_launch();
         return;
     }
