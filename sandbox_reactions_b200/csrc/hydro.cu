@@ -12,7 +12,10 @@
 
 #include <cudaTypedefs.h>
 
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 
 #include "tma.cuh"
 
@@ -591,6 +594,19 @@ size_t hydro_smem_bytes() { return sizeof(BandShared); }
 int hydro_blocks(int w, int h) { return (int)(div_up(w, HB_TX) * div_up(h, HB_TY)); }
 
 void tma_encode_planes(CUtensorMap* map, const float* base, int w, int h, int planes, int bx, int by) {
+    // encoded maps are kept by their arguments: a launch on the same planes (every launch of a step, every smoother
+    // launch of a level) copies its map instead of paying the driver call before the launch
+    static std::mutex mu;
+    static std::map<std::tuple<const float*, int, int, int, int, int>, CUtensorMap> cache;
+    const auto key = std::make_tuple(base, w, h, planes, bx, by);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        const auto it = cache.find(key);
+        if (it != cache.end()) {
+            *map = it->second;
+            return;
+        }
+    }
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     if (!encode) {
         void* fn = nullptr;
@@ -608,6 +624,9 @@ void tma_encode_planes(CUtensorMap* map, const float* base, int w, int h, int pl
                               unit, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw SrError{SR_E_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r)};
+    std::lock_guard<std::mutex> lock(mu);
+    if (cache.size() > 4096) cache.clear();
+    cache[key] = *map;
 }
 
 template <int MODE, int LIM, bool BRACKET>
