@@ -26,7 +26,8 @@ __global__ void box_cells_kernel(const float* __restrict__ sigma, int w, int h, 
     int x0 = INT_MAX, y0 = INT_MAX, x1 = INT_MIN, y1 = INT_MIN;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (sigma[i] >= sigma_vac) {
-            const int x = (int)(i % w), y = (int)(i / w);
+            int x, y;
+            split_index(i, w, x, y);
             x0 = min(x0, x);
             y0 = min(y0, y);
             x1 = max(x1, x + 1);

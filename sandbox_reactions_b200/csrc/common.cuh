@@ -133,6 +133,14 @@ SR_HOST_DEVICE void euler_flux(const Prim& p, float energy, int dir, float* f) {
     f[3] = (energy + p.p) * un;
 }
 
+// x = i mod w, y = i / w for a cell or face index below 2^32 (every world here), by 32-bit division: the 64-bit
+// division of a size_t index costs an emulated sequence per element in the grid-stride kernels.
+SR_HOST_DEVICE void split_index(size_t i, int w, int& x, int& y) {
+    const unsigned u = (unsigned)i, uw = (unsigned)w;
+    y = (int)(u / uw);
+    x = (int)(u - (unsigned)y * uw);
+}
+
 // ------------------------------------------------------------------------------------------------ launch helpers
 // Every kernel launch of the library is counted (sr_cost.kernel_launches reports the count of an sr_step call).
 // The message sr_last_error(NULL) returns (calls without a context).

@@ -240,7 +240,8 @@ __global__ void grav_gradient_kernel(GravArgs A) {
     const int w = A.w, h = A.h, rw = w + 2;
     const size_t n = (size_t)w * h;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         const float* r0 = A.phi_ring + (size_t)y * rw;
         const float* r1 = r0 + rw;
         const float* r2 = r1 + rw;

@@ -220,7 +220,8 @@ __global__ void heat_faces_kernel(HeatConst K, const uint8_t* __restrict__ gas, 
         Side a, b;
         bool ha, hb;
         if (f < nx) {
-            const int x = (int)(f % (w + 1)), y = (int)(f / (w + 1));
+            int x, y;
+            split_index(f, (w + 1), x, y);
             ha = x > 0;
             hb = x < w;
             if (ha) a = side_at(K, gas, t0, kap, sig, C, (size_t)y * w + x - 1);
@@ -228,7 +229,8 @@ __global__ void heat_faces_kernel(HeatConst K, const uint8_t* __restrict__ gas, 
             kx[f] = face_coef(K, ha ? &a : nullptr, hb ? &b : nullptr);
         } else {
             const size_t g = f - nx;
-            const int x = (int)(g % w), y = (int)(g / w);
+            int x, y;
+            split_index(g, w, x, y);
             ha = y > 0;
             hb = y < h;
             if (ha) a = side_at(K, gas, t0, kap, sig, C, (size_t)(y - 1) * w + x);
@@ -248,7 +250,8 @@ __global__ void heat_ksum_kernel(HeatConst K, const uint8_t* __restrict__ gas, c
             kvac[i] = 0.0;
             continue;
         }
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         const double k[4] = {kx[(size_t)y * (w + 1) + x], kx[(size_t)y * (w + 1) + x + 1], ky[(size_t)y * w + x],
                              ky[(size_t)(y + 1) * w + x]};
         const bool nb[4] = {x > 0 && gas[i - 1], x + 1 < w && gas[i + 1], y > 0 && gas[i - w],
@@ -316,7 +319,8 @@ __global__ void heat_residual64_kernel(HeatConst K, const double* __restrict__ s
         for (int u = 0; u < 2; u++) {
             const size_t i = base + u * stride;
             if (i >= n) break;
-            const int xx = (int)(i % w), y = (int)(i / w);
+            int xx, y;
+            split_index(i, w, xx, y);
             const bool gi = gas[i];
             const bool gl = xx > 0 && gas[i - 1], gr = xx + 1 < w && gas[i + 1];
             const bool gu = y > 0 && gas[i - w], gd = y + 1 < h && gas[i + w];
@@ -386,7 +390,8 @@ __global__ void spmv_kernel(MgLevel L, const float* __restrict__ p, float* __res
             pv[u] = 0.0f;
             v[u] = 0.0f;
             if (i < n) {
-                const int x = (int)(i % w), y = (int)(i / w);
+                int x, y;
+                split_index(i, w, x, y);
                 const float pi = p[i];
                 const float pl = x > 0 ? p[i - 1] : pi, pr = x + 1 < w ? p[i + 1] : pi;
                 const float pu = y > 0 ? p[i - w] : pi, pd = y + 1 < h ? p[i + w] : pi;
@@ -486,7 +491,8 @@ __global__ void spmv_dir_kernel(MgLevel L, const double* __restrict__ scal, cons
     double acc = 0.0;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += stride) {
         const size_t i = 4 * t;
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         auto pn4 = [&](size_t j) {
             const float4 zz = *reinterpret_cast<const float4*>(z + j);
             if (first) return zz;
@@ -584,7 +590,8 @@ __global__ void vcycle_residual_kernel(MgLevel L, const float* __restrict__ r, c
     const int w = L.w, h = L.h;
     const size_t n = (size_t)w * h;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         float v = 0.0f;
         const float zi = z[i];
         if (L.mask[i]) {
@@ -606,7 +613,8 @@ __global__ void jacobi_kernel(MgLevel L, const float* __restrict__ r, float* z, 
     const size_t n = (size_t)w * h;
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         const float dl = x > 0 ? L.dx[i - 1] : 0.0f, du = y > 0 ? L.dy[i - w] : 0.0f;
         const float zi = L.mask[i] ? r[i] / (L.c[i] + dl + L.dx[i] + du + L.dy[i]) : 0.0f;
         z[i] = zi;
@@ -709,13 +717,15 @@ __global__ void heat_flux_kernel(HeatConst K, const uint8_t* __restrict__ gas, c
         long a, b;
         double k;
         if (f < nx) {
-            const int x = (int)(f % (w + 1)), y = (int)(f / (w + 1));
+            int x, y;
+            split_index(f, (w + 1), x, y);
             a = x > 0 ? (long)y * w + x - 1 : -1;
             b = x < w ? (long)y * w + x : -1;
             k = kx[f];
         } else {
             const size_t g = f - nx;
-            const int x = (int)(g % w), y = (int)(g / w);
+            int x, y;
+            split_index(g, w, x, y);
             a = y > 0 ? (long)(y - 1) * w + x : -1;
             b = y < h ? (long)y * w + x : -1;
             k = ky[g];
@@ -792,7 +802,8 @@ __global__ void limited_scale_kernel(HeatConst K, const double* __restrict__ sca
             scale[i] = 1.0;
             continue;
         }
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         const long L = x > 0 ? (long)i - 1 : -1, R = x + 1 < w ? (long)i + 1 : -1;
         const long Uu = y > 0 ? (long)i - w : -1, D = y + 1 < h ? (long)i + w : -1;
         const double lv[4] = {-face_flux(K, gas, u, kx[(size_t)y * (w + 1) + x], L, (long)i, u_vac),
@@ -819,7 +830,8 @@ __global__ void limited_apply_kernel(HeatConst K, const double* __restrict__ sca
     double rad = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         if (!gas[i]) continue;
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         const long nb[4] = {x > 0 ? (long)i - 1 : -1, x + 1 < w ? (long)i + 1 : -1, y > 0 ? (long)i - w : -1,
                             y + 1 < h ? (long)i + w : -1};
         double F[4] = {face_flux(K, gas, u, kx[(size_t)y * (w + 1) + x], nb[0], (long)i, u_vac),

@@ -846,7 +846,8 @@ __global__ void ref_apply_kernel(RefArgs A) {
             changed = true;
         }
         if (!A.held[i] && A.Uout[i] >= R.sigma_vac) {
-            const int x = (int)(i % w), y = (int)(i / w);
+            int x, y;
+            split_index(i, w, x, y);
             const bool into_x = (x > 0 && A.held[i - 1] && mx < 0.0f) || (x + 1 < w && A.held[i + 1] && mx > 0.0f);
             const bool into_y = (y > 0 && A.held[i - w] && my < 0.0f) || (y + 1 < h && A.held[i + w] && my > 0.0f);
             if (into_x) {
@@ -948,7 +949,9 @@ __global__ void ref_hold_dt_kernel(RefConst R, float* __restrict__ U, uint8_t* _
                 bool now = false;
                 if (rest) {
                     // the mass of the disk r <= r_hold about the cell, centre to centre, clipped (sinks.rs:117-125)
-                    const int k = (int)R.r_hold, x0 = (int)(i % w), y0 = (int)(i / w);
+                    const int k = (int)R.r_hold;
+                    int x0, y0;
+                    split_index(i, w, x0, y0);
                     const float r2 = R.r_hold * R.r_hold;
                     double m = 0.0;
                     for (int dy = -k; dy <= k; dy++) {

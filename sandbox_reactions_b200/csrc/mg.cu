@@ -44,7 +44,8 @@ __global__ void mg_couplings0_kernel(MgLevel L, const double* __restrict__ kx, c
     const int w = L.w, h = L.h;
     const size_t n = (size_t)w * h;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % w), y = (int)(i / w);
+        int x, y;
+        split_index(i, w, x, y);
         const bool g = gas[i];
         L.mask[i] = g;
         L.dx[i] = (g && x + 1 < w && gas[i + 1]) ? (float)kx[(size_t)y * (w + 1) + x + 1] : 0.0f;
@@ -1291,7 +1292,7 @@ void Multigrid::create(int w, int h, int pre_, int post_) {
             SR_CUDA_TRY(cudaMalloc(&L.x2, n * sizeof(float)));
         }
         nlevels++;
-        if ((lw <= 8 && lh <= 8) || nlevels == kMgMaxLevels) break;
+        if ((lw <= 4 && lh <= 4) || nlevels == kMgMaxLevels) break;
         lw = (lw + 1) / 2;
         lh = (lh + 1) / 2;
     }

@@ -11,7 +11,7 @@
 // (global parity), V(pre, post), the post-smoother sweeping the colours in reverse so the cycle is symmetric. Big
 // levels run as tile kernels that do all of a smoother's half-sweeps in shared memory (temporal blocking: the tile's
 // halo is as deep as the half-sweeps); every level of at most kMgTailCells cells runs inside one CTA (the coarse tail,
-// the reference's mg_coarse), and the coarsest level (at most 8 x 8) is solved exactly by its inverse, built once per
+// the reference's mg_coarse), and the coarsest level (at most 4 x 4) is solved exactly by its inverse, built once per
 // Newton pass.
 #pragma once
 
