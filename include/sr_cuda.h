@@ -187,7 +187,8 @@ sr_status sr_step(sr_ctx* ctx, uint32_t steps);
 sr_status sr_read_dt(sr_ctx* ctx, sr_dt_report* out);
 /* Step::read_heat (step/heat.rs:499-512). */
 sr_status sr_read_heat(sr_ctx* ctx, sr_heat_report* out);
-/* Step::gravity_field (step/mod.rs:532-534): P2's field of the state the last step started from; W*H each. */
+/* Step::gravity_field (step/mod.rs:532-534): P2's field of the state the last step started from; W*H each. With the
+ * active box, P2 runs over the box: its field inside the box, 0 outside. */
 sr_status sr_gravity_field(sr_ctx* ctx, float* gx, float* gy, float* phi);
 /* Step::read_heat_flux (step/heat.rs:542-548): the last implicit step's solved face fluxes, (W+1)*H and W*(H+1). */
 sr_status sr_heat_flux(sr_ctx* ctx, float* fx, float* fy);

@@ -973,11 +973,26 @@ sr_status sr_read_heat(sr_ctx* c, sr_heat_report* out) {
 sr_status sr_gravity_field(sr_ctx* c, float* gx, float* gy, float* phi) {
     return guarded(c, [&] {
         SR_REQUIRE(c->cfg.gravity, "sr_gravity_field: the context runs no gravity pass");
-        if (c->sub) {  // P2 of the world's state as it stands
-            box_sync(c);
-            c->grav.solve(planes(c), c->phi, c->gx, c->gy, c->stream);
-        }
         SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (c->sub) {
+            // the box's P2 (the field of the last step's start state over the box, as the reference's box-sized P2
+            // leaves it), 0 outside the box
+            sr_ctx* s = c->sub;
+            const BoxRec& b = c->box;
+            SR_CUDA_TRY(cudaStreamSynchronize(s->stream));
+            std::vector<float> crop(s->n);
+            float* outs[3] = {gx, gy, phi};
+            const float* srcs[3] = {s->gx, s->gy, s->phi};
+            for (int k = 0; k < 3; k++) {
+                if (!outs[k]) continue;
+                SR_CUDA_TRY(cudaMemcpy(crop.data(), srcs[k], sizeof(float) * s->n, cudaMemcpyDeviceToHost));
+                std::fill(outs[k], outs[k] + c->n, 0.0f);
+                for (int y = 0; y < b.h; y++)
+                    std::copy(crop.data() + (size_t)y * b.w, crop.data() + (size_t)(y + 1) * b.w,
+                              outs[k] + (size_t)(y + b.y0) * c->w + b.x0);
+            }
+            return;
+        }
         if (gx) SR_CUDA_TRY(cudaMemcpy(gx, c->gx, sizeof(float) * c->n, cudaMemcpyDeviceToHost));
         if (gy) SR_CUDA_TRY(cudaMemcpy(gy, c->gy, sizeof(float) * c->n, cudaMemcpyDeviceToHost));
         if (phi) SR_CUDA_TRY(cudaMemcpy(phi, c->phi, sizeof(float) * c->n, cudaMemcpyDeviceToHost));

@@ -152,3 +152,28 @@ def test_the_box_steps_faster_than_the_whole_world():
             s.run(16)
             ms[box] = s.read_cost().total_ms
     assert ms[True] * 4.0 < ms[False], ms
+
+
+def test_the_boxed_world_answers_the_reads_of_the_whole_world():
+    # heat on: the implicit step's report and face fluxes (the world's face planes, 0 outside the box), P2's field
+    # inside the box, the clock; against the same world stepped whole
+    cfg, P = disk_world(256, r=36.0, vr=0.3, t=20.0)
+    cfg = cfg.replace(heat=True, opacity_plane=True, mu=1.0)
+    rng = np.random.default_rng(4)
+    kappa = (1.0 + 0.5 * rng.random((256, 256))).astype(np.float32)
+    got = {}
+    for box in (False, True):
+        with Step(cfg.replace(active_box=box)) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            s.run(5)
+            got[box] = (s.read_heat(), s.read_heat_flux(), s.gravity_field(), s.read_dt(), s.read_box())
+    (hw, fw, gw, dw, _), (hb, fb, gb, db, b) = got[False], got[True]
+    assert hw.converged and hb.converged and hb.rel_residual <= 1e-8
+    assert abs(db.sim_time - dw.sim_time) <= 1e-6 * dw.sim_time and db.steps == dw.steps == 5
+    for k in range(2):
+        assert rel_l1(fb[k], fw[k]) <= 1e-4, (k, rel_l1(fb[k], fw[k]))
+    ys, xs = slice(b.y0, b.y0 + b.h), slice(b.x0, b.x0 + b.w)
+    for k in range(3):
+        assert rel_l1(gb[k][ys, xs], gw[k][ys, xs]) <= 1e-5, (k, rel_l1(gb[k][ys, xs], gw[k][ys, xs]))
+        assert np.all(gb[k][:b.y0] == 0.0) and np.all(gb[k][b.y0 + b.h:] == 0.0)
