@@ -7,10 +7,10 @@ seeded synthetic world of S x S cells (default 2048): a Gaussian disk with logno
 lognormal opacity field with a 32-cell correlation length over six decades, hot spots in the gas (scenes.full_step).
 Under torchrun every rank advances its own world (scene seed = rank): the worlds are independent, no collective on the
 data path, weak scaling. The line also carries: the FLD time-to-1e-8 of the 2048² implicit-diffusion configuration
-(scenes.fld) with plain MG-PCG, Jacobi-PCG and the learned preconditioner; the other single-GPU configurations (Sod
-512², the 1024² disk) with their parity against the oracle; the full-size parity of one step against the f64 twin;
-and config 5, 64 worlds of a seeded 256²…2048² mix advanced as one captured graph per batch step against the same
-worlds one at a time (`batched`).
+(scenes.fld) with plain MG-PCG (its V(2,2), and V(4,4) as the full step runs it), Jacobi-PCG and the learned
+preconditioner; the other single-GPU configurations (Sod 512², the 1024² disk) with their parity against the oracle;
+the full-size parity of one step against the f64 twin; and config 5, 64 worlds of a seeded 256²…2048² mix advanced
+as one captured graph per batch step against the same worlds one at a time (`batched`).
 
 `--impl reference` times the reference's own CPU algorithm (the f64 twin restated in C, oracle/) on the same 2048²
 world with every host thread, for as many of the K steps as fit a bounded time (at least one), and beside it one
@@ -18,10 +18,10 @@ thread on a 512² sample of the scene.
 
 `--case fld|full|learned|sod|grav --size S` runs one small self-contained workload per hot kernel family instead (what
 the committed ncu summaries were captured on) and prints one line with its device time: fld, the implicit-diffusion
-world's first system solved to 1e-8 `--solves` times (smoothers, coarse tail, SpMV, PCG vectors); full, `--steps` full
-steps of the benchmark world; learned, one flexible-CG round with an untrained learned preconditioner (the convolution
-kernels' cost does not depend on the weights); sod, `--steps` hydro-only steps of a Sod tube (the stencil kernel);
-grav, `--solves` gravity-only steps of a disk (the FFT kernels).
+world's first system solved to 1e-8 `--solves` times (smoothers, coarse tail, SpMV, PCG vectors; `--sweeps 4` for
+V(4,4)); full, `--steps` full steps of the benchmark world; learned, one flexible-CG round with an untrained learned
+preconditioner (the convolution kernels' cost does not depend on the weights); sod, `--steps` hydro-only steps of a
+Sod tube (the stencil kernel); grav, `--solves` gravity-only steps of a disk (the FFT kernels).
 """
 from __future__ import annotations
 
@@ -219,12 +219,15 @@ def run_case(args, local):
     n = args.size
     if args.case == "fld":
         cfg, P, kappa = scenes.fld(n)
+        if args.sweeps:
+            cfg = cfg.replace(mg_pre=args.sweeps, mg_post=args.sweeps)
         with Step(cfg) as s:
             s.upload(P)
             s.upload_opacity(kappa)
             for _ in range(args.solves):
                 ms, rounds, rel, _ = s.heat_first_solve(cfg.dt_fixed, args.precond)
-        print(f"fld {n}: {args.precond} first solve {ms:.3f} ms, {rounds} rounds, rel residual {rel:.2e}")
+        print(f"fld {n}: {args.precond} first solve V({cfg.mg_pre},{cfg.mg_post}) {ms:.3f} ms, {rounds} rounds, "
+              f"rel residual {rel:.2e}")
     elif args.case == "full":
         cfg, P, kappa = scenes.full_step(n)
         with Step(cfg) as s:
@@ -315,6 +318,13 @@ def fld_time_to_tol(size: int):
             except SrError as e:
                 out[pc] = {"unavailable": e.message}
         s.attach_learner(None)
+    # the same system with the full step's V(4,4) (the configuration names V(2,2))
+    with Step(cfg.replace(mg_pre=4, mg_post=4)) as s:
+        s.upload(P)
+        s.upload_opacity(kappa)
+        s.heat_first_solve(cfg.dt_fixed, "mg")
+        ms, rounds, rel, _ = s.heat_first_solve(cfg.dt_fixed, "mg")
+        out["mg_v44"] = {"ms": ms, "rounds": rounds, "rel_residual": rel}
     if learner is not None:
         learner.close()
     if "ms" in out.get("learned", {}) and "ms" in out.get("mg", {}):
@@ -564,6 +574,8 @@ def main():
                     help="run one profiling workload instead of the benchmark")
     ap.add_argument("--solves", type=int, default=3)
     ap.add_argument("--precond", default="mg")
+    ap.add_argument("--sweeps", type=int, default=0,
+                    help="--case fld: red-black sweeps a side of the V-cycle (0: the configuration's V(2,2))")
     ap.add_argument("--no-fld", action="store_true", help="skip the FLD time-to-1e-8 measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-world batch (config 5) side measurement")
     ap.add_argument("--no-box", action="store_true", help="skip the active box side measurement")

@@ -71,7 +71,7 @@ typedef struct sr_config {
     uint32_t precond;         /* SR_PRECOND_* */
     uint32_t flux_limiter;    /* 1: Levermore-Pomraning λ(R); 0: λ = 1/3 (heat.rs TestFlags) */
     uint32_t opacity_plane;   /* 1: κ per cell from sr_upload_opacity; 0: κ = kappa0 everywhere */
-    uint32_t mg_pre, mg_post; /* red-black sweeps before / after the coarse correction: V(mg_pre, mg_post) */
+    uint32_t mg_pre, mg_post; /* red-black sweeps before / after the coarse correction: V(mg_pre, mg_post), 1..4 */
     uint32_t max_passes;      /* Newton passes per implicit step (reference heat.rs:51 MAX_PASSES = 128) */
     uint32_t max_rounds;      /* PCG rounds over all passes (heat.rs:52 MAX_ROUNDS = 4096) */
     uint32_t pin_temperature; /* heat.rs TestFlags::pin_temperature */

@@ -79,8 +79,8 @@ class Config:
     precond: str = "mg"
     flux_limiter: bool = True
     opacity_plane: bool = False
-    mg_pre: int = 2
-    mg_post: int = 2
+    mg_pre: int = 4
+    mg_post: int = 4
     max_passes: int = 128
     max_rounds: int = 4096
     pin_temperature: bool = False

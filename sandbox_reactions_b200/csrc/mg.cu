@@ -1222,11 +1222,13 @@ void smooth(int nu, bool pre, const MgLevel& L, const MgLevel& C, const float* x
     if (pre) {
         if (nu == 1) launch_smooth<2, true>(L, C, xc, omega, part, counter, out, tile, s);
         else if (nu == 2) launch_smooth<4, true>(L, C, xc, omega, part, counter, out, tile, s);
-        else launch_smooth<6, true>(L, C, xc, omega, part, counter, out, tile, s);
+        else if (nu == 3) launch_smooth<6, true>(L, C, xc, omega, part, counter, out, tile, s);
+        else launch_smooth<8, true>(L, C, xc, omega, part, counter, out, tile, s);
     } else {
         if (nu == 1) launch_smooth<2, false>(L, C, xc, omega, part, counter, out, tile, s);
         else if (nu == 2) launch_smooth<4, false>(L, C, xc, omega, part, counter, out, tile, s);
-        else launch_smooth<6, false>(L, C, xc, omega, part, counter, out, tile, s);
+        else if (nu == 3) launch_smooth<6, false>(L, C, xc, omega, part, counter, out, tile, s);
+        else launch_smooth<8, false>(L, C, xc, omega, part, counter, out, tile, s);
     }
 }
 
@@ -1264,14 +1266,14 @@ size_t mg_smooth_ctas(int w, int h) {
     MgLevel L;
     L.w = w;
     L.h = h;
-    // a bound: the shortest tile tile_sy can pick, or the row-band kernel's smallest output tile (V(3,3)'s pre-smoother)
-    const size_t rb = (size_t)div_up(w, RB_RX - 2 * rb_halo<6, true>()) * div_up(h, RB_RY - 2 * rb_halo<6, true>());
+    // a bound: the shortest tile tile_sy can pick, or the row-band kernel's smallest output tile (V(4,4)'s pre-smoother)
+    const size_t rb = (size_t)div_up(w, RB_RX - 2 * rb_halo<8, true>()) * div_up(h, RB_RY - 2 * rb_halo<8, true>());
     return std::max(rb, small_tiles(L) ? (size_t)div_up(w, SMALL_SX) * div_up(h, SMALL_SY - 6)
                                        : (size_t)div_up(w, BIG_SX) * div_up(h, BIG_SY - 6));
 }
 
 void Multigrid::create(int w, int h, int pre_, int post_) {
-    SR_REQUIRE(pre_ >= 1 && pre_ <= 3 && post_ >= 1 && post_ <= 3, "V-cycle sweeps must be 1..3");
+    SR_REQUIRE(pre_ >= 1 && pre_ <= 4 && post_ >= 1 && post_ <= 4, "V-cycle sweeps must be 1..4");
     pre = pre_;
     post = post_;
     nlevels = 0;
@@ -1313,6 +1315,7 @@ void Multigrid::create(int w, int h, int pre_, int post_) {
     set_attributes_ns<2>();
     set_attributes_ns<4>();
     set_attributes_ns<6>();
+    set_attributes_ns<8>();
 }
 
 void Multigrid::destroy() {

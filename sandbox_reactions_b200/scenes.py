@@ -113,7 +113,7 @@ def fld(n: int = 2048, scene: int = 0, dt_factor: float = 50.0):
     T = hot_spots(n, rng, 1e3, 1e6)
     sigma = np.ones((n, n))
     cfg = Config(width=n, height=n, hydro=False, gravity=False, heat=True, opacity_plane=True, gamma=gamma, mu=mu,
-                 edge="bounce")
+                 edge="bounce", mg_pre=2, mg_post=2)  # the configuration's preconditioner: V(2,2)
     dt = dt_factor * explicit_limit(cfg, T, sigma, kappa.astype(np.float64))
     cfg = cfg.replace(dt_fixed=dt)
     z = np.zeros((n, n))

@@ -138,3 +138,38 @@ def test_one_full_step_with_every_pass_matches_the_twin():
     ref = twin.state()
     for k in range(4):
         assert rel_l1(gpu[k], ref[k]) <= 1e-5, (k, rel_l1(gpu[k], ref[k]))
+
+
+@pytest.mark.parametrize("pre,post", [(1, 1), (2, 2), (3, 3), (4, 4), (2, 4), (4, 1)])
+def test_every_v_cycle_solves_the_first_system(pre, post):
+    # 1..4 red-black sweeps a side (the smoothers' 2..8 half-sweep instances): the same solution to 1e-8, the deeper
+    # cycles in no more rounds than V(1,1)
+    cfg, P, kappa = scenes.fld(128, scene=7)
+    cfg = cfg.replace(mg_pre=pre, mg_post=post)
+    diag, rhs, kx, ky, gas = O.heat_system(cfg, P.astype(np.float64), cfg.dt_fixed, kappa.astype(np.float64))
+    x_ref, _ = O.heat_pcg(diag, rhs, kx, ky, gas, rel=1e-12, max_rounds=200000)
+    with Step(cfg) as s:
+        s.upload(P)
+        s.upload_opacity(kappa)
+        _, rounds, rel, x = s.heat_first_solve(cfg.dt_fixed, "mg", want_x=True)
+        with Step(cfg.replace(mg_pre=1, mg_post=1)) as s1:
+            s1.upload(P)
+            s1.upload_opacity(kappa)
+            _, rounds1, _, _ = s1.heat_first_solve(cfg.dt_fixed, "mg")
+    assert rel <= 1e-8 and rounds <= rounds1, (rounds, rounds1)
+    assert np.abs(x - x_ref).max() <= 1e-6 * np.abs(x_ref).max()
+
+
+def test_v44_on_the_row_band_levels():
+    # a 1024² world: its big levels take the row-band smoothers (V(4,4): the 8 half-sweep instances, halos 10 and 8)
+    cfg, P, kappa = scenes.fld(1024, scene=9)
+    got = {}
+    for nu in (2, 4):
+        with Step(cfg.replace(mg_pre=nu, mg_post=nu)) as s:
+            s.upload(P)
+            s.upload_opacity(kappa)
+            _, rounds, rel, x = s.heat_first_solve(cfg.dt_fixed, "mg", want_x=True)
+        assert rel <= 1e-8
+        got[nu] = (rounds, x)
+    assert got[4][0] <= got[2][0]
+    assert np.abs(got[4][1] - got[2][1]).max() <= 1e-6 * np.abs(got[2][1]).max()
