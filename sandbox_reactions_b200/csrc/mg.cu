@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -1372,13 +1373,13 @@ constexpr float kTuneMargin = 0.95f;
 
 void Multigrid::autotune(cudaStream_t s) {
     static std::mutex mu;
-    static std::map<std::pair<int, int>, int> chosen;
+    static std::map<std::tuple<int, int, int, int>, int> chosen;  // (w, h, sweeps before, after) -> tile
     tuned = true;
     cudaEvent_t a, b;
     SR_CUDA_TRY(cudaEventCreate(&a));
     SR_CUDA_TRY(cudaEventCreate(&b));
     for (int l = 1; l < tail; l++) {
-        const std::pair<int, int> key(L[l].w, L[l].h);
+        const std::tuple<int, int, int, int> key(L[l].w, L[l].h, pre, post);
         {
             std::lock_guard<std::mutex> g(mu);
             auto it = chosen.find(key);
