@@ -646,31 +646,45 @@ def main():
     # the dominant kernels, timed live on the library's stream with CUDA events (L2 flushed before each launch)
     pre_ms, post_ms = step.time_smoother(10)
 
-    # ---- end to end through the C ABI: per step the state and κ from pinned host memory in, the state out
+    # ---- end to end through the C ABI: per step the run's resumable state from pinned host memory in — the cells, κ
+    # and P5's rate (the next step's first iterate, which a dump carries) — and the cells and the rate out; beside it
+    # the cells and κ alone, each step then starting its implicit solve cold (sr_upload zeroes the rate)
     pin_in = torch.empty((4, n, n), dtype=torch.float32, pin_memory=True)
     pin_k = torch.empty((n, n), dtype=torch.float32, pin_memory=True)
     pin_out = torch.empty((4, n, n), dtype=torch.float32, pin_memory=True)
+    pin_rate = torch.empty((n, n), dtype=torch.float32, pin_memory=True)
     step.readback(pin_in.numpy())  # the state the timed steps left: the end-to-end steps continue from it
+    step.read_heat_rate(pin_rate.numpy())
     pin_k.numpy()[...] = kappa
     e2e_steps = max(1, min(args.steps, 5))
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0.record()
-    for k in range(e2e_steps):
-        src, dst = (pin_in, pin_out) if k % 2 == 0 else (pin_out, pin_in)
-        step.upload(src.numpy())
-        step.upload_opacity(pin_k.numpy())
-        step.run(1)
-        step.readback(dst.numpy())
-    ev1.record()
-    torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * n * n * e2e_steps / (float(t.item()) / 1e3) / 1e6
+    bufs = [pin_in, pin_out]
+
+    def e2e_leg(with_rate: bool) -> float:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(e2e_steps):
+            src, dst = bufs
+            bufs.reverse()  # this step's result is the next step's input
+            step.upload(src.numpy())
+            step.upload_opacity(pin_k.numpy())
+            if with_rate:
+                step.set_heat_rate(pin_rate.numpy())
+            step.run(1)
+            step.readback(dst.numpy())
+            if with_rate:
+                step.read_heat_rate(pin_rate.numpy())
+        ev1.record()
+        torch.cuda.synchronize()
+        t = torch.tensor([ev0.elapsed_time(ev1)], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return world * n * n * e2e_steps / (float(t.item()) / 1e3) / 1e6
+
+    e2e_value = e2e_leg(True)
+    e2e_cold = e2e_leg(False)
 
     cpu = parity = None
     if rank == 0 and world == 1:
@@ -723,8 +737,13 @@ def main():
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(n, world),
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 5 * 4 * n * n,
-                    "d2h_bytes_per_step": 4 * 4 * n * n, "steps": e2e_steps},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 6 * 4 * n * n,
+                    "d2h_bytes_per_step": 5 * 4 * n * n, "steps": e2e_steps,
+                    "what": "per step through the C ABI: the cells, κ and P5's rate in from pinned host memory, the "
+                            "cells and the rate out (the run's resumable state, as a dump carries it)",
+                    "cells_only": {"value": e2e_cold, "h2d_bytes_per_step": 5 * 4 * n * n,
+                                   "d2h_bytes_per_step": 4 * 4 * n * n,
+                                   "what": "the cells and κ in, the cells out: each step's implicit solve starts cold"}},
             "gpu_launches": int(cost.kernel_launches),
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -175,6 +175,11 @@ extern "C" {
     pub fn sr_read_heat(ctx: *mut sr_ctx, out: *mut sr_heat_report) -> sr_status;
     pub fn sr_gravity_field(ctx: *mut sr_ctx, gx: *mut f32, gy: *mut f32, phi: *mut f32) -> sr_status;
     pub fn sr_heat_flux(ctx: *mut sr_ctx, fx: *mut f32, fy: *mut f32) -> sr_status;
+    pub fn sr_set_clock(ctx: *mut sr_ctx, steps: u64, sim_time: f64, dt: f64, dt_next: f64) -> sr_status;
+    pub fn sr_read_heat_rate(ctx: *mut sr_ctx, rate: *mut f32) -> sr_status;
+    pub fn sr_set_heat_rate(ctx: *mut sr_ctx, rate: *const f32) -> sr_status;
+    pub fn sr_read_side_flux(ctx: *mut sr_ctx, fx: *mut f32, fy: *mut f32) -> sr_status;
+    pub fn sr_set_side_flux(ctx: *mut sr_ctx, fx: *const f32, fy: *const f32) -> sr_status;
     pub fn sr_set_edge_mode(ctx: *mut sr_ctx, edge: u32) -> sr_status;
     pub fn sr_set_heat_precond(ctx: *mut sr_ctx, precond: u32) -> sr_status;
     pub fn sr_set_heat_limits(ctx: *mut sr_ctx, max_passes: u32, max_rounds: u32) -> sr_status;
@@ -283,6 +288,41 @@ impl Step {
     pub fn upload_opacity(&mut self, kappa: &[f32]) -> Result<(), Error> {
         assert_eq!(kappa.len(), self.plane_len(), "one plane of width x height");
         self.check(unsafe { sr_upload_opacity(self.ctx, kappa.as_ptr()) })
+    }
+
+    /// `Step::restore` (step/latch.rs:493-510): the next step's index, the sim time, Δt_n and the next Δt.
+    pub fn set_clock(&mut self, steps: u64, sim_time: f64, dt: f64, dt_next: f64) -> Result<(), Error> {
+        self.check(unsafe { sr_set_clock(self.ctx, steps, sim_time, dt, dt_next) })
+    }
+
+    /// `Step::heat_rate` (step/heat.rs:550-565): each cell's P5 rate of the last step.
+    pub fn heat_rate(&mut self, rate: &mut [f32]) -> Result<(), Error> {
+        assert_eq!(rate.len(), self.plane_len(), "one plane of width x height");
+        self.check(unsafe { sr_read_heat_rate(self.ctx, rate.as_mut_ptr()) })
+    }
+
+    /// `Step::set_heat_rate` (step/heat.rs:566-582): a dump's rate, or zeros for None.
+    pub fn set_heat_rate(&mut self, rate: Option<&[f32]>) -> Result<(), Error> {
+        let ptr = match rate {
+            Some(r) => {
+                assert_eq!(r.len(), self.plane_len(), "one plane of width x height");
+                r.as_ptr()
+            }
+            None => std::ptr::null(),
+        };
+        self.check(unsafe { sr_set_heat_rate(self.ctx, ptr) })
+    }
+
+    /// `Step::side_flux` (step/heat.rs:584-589), read back: the cell-centred F the next P4 pushes with.
+    pub fn side_flux(&mut self, fx: &mut [f32], fy: &mut [f32]) -> Result<(), Error> {
+        assert!(fx.len() == self.plane_len() && fy.len() == self.plane_len(), "one plane of width x height each");
+        self.check(unsafe { sr_read_side_flux(self.ctx, fx.as_mut_ptr(), fy.as_mut_ptr()) })
+    }
+
+    /// `load_dump`'s write of F into the step's side flux (dump.rs:404-407).
+    pub fn set_side_flux(&mut self, fx: &[f32], fy: &[f32]) -> Result<(), Error> {
+        assert!(fx.len() == self.plane_len() && fy.len() == self.plane_len(), "one plane of width x height each");
+        self.check(unsafe { sr_set_side_flux(self.ctx, fx.as_ptr(), fy.as_ptr()) })
     }
 
     /// `Step::run` (step/mod.rs:703-718).

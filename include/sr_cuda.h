@@ -193,6 +193,23 @@ sr_status sr_gravity_field(sr_ctx* ctx, float* gx, float* gy, float* phi);
 /* Step::read_heat_flux (step/heat.rs:542-548): the last implicit step's solved face fluxes, (W+1)*H and W*(H+1). */
 sr_status sr_heat_flux(sr_ctx* ctx, float* fx, float* fy);
 
+/* The records a state dump carries beyond the cells, for resuming a run where it stopped (dump_state / load_dump,
+ * crates/sr-engine/src/dump.rs:355-410). sr_set_clock is Step::restore (step/latch.rs:493-510): the next step's index
+ * is `steps`, the sim time goes on from `sim_time`, Δt_n = dt and the next step's Δt = dt_next, the guard's finding
+ * cleared. sr_upload resets the clock, so the resume calls follow it. With the active box the box stays the one fit at
+ * the upload and the refits follow the restored step index. */
+sr_status sr_set_clock(sr_ctx* ctx, uint64_t steps, double sim_time, double dt, double dt_next);
+/* Step::heat_rate / set_heat_rate (step/heat.rs:550-582): each cell's P5 rate (T − T⁰)/Δt in the last step, W*H f32
+ * row-major — the next step's first iterate is T⁰ + rate·Δt. sr_upload zeroes it; sr_set_heat_rate after the upload
+ * restores a dump's (NULL: zeros). The context must run P5. */
+sr_status sr_read_heat_rate(sr_ctx* ctx, float* rate);
+sr_status sr_set_heat_rate(sr_ctx* ctx, const float* rate);
+/* Step::side_flux (step/heat.rs:584-589): the cell-centred F (F_x and F_y, W*H f32 each) that the next step's P4
+ * pushes with — reference mode with P5 only (channels 14, heat on). sr_upload zeroes it (the first step takes no
+ * radiation force, reference/mod.rs:122-123); sr_set_side_flux after the upload restores a dump's. */
+sr_status sr_read_side_flux(sr_ctx* ctx, float* fx, float* fy);
+sr_status sr_set_side_flux(sr_ctx* ctx, const float* fx, const float* fy);
+
 /* Step::set_edge_mode (step/mod.rs:544-548). */
 sr_status sr_set_edge_mode(sr_ctx* ctx, uint32_t edge);
 /* Step::set_heat_precond (step/heat.rs:595-599). */

@@ -6,6 +6,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
 #include <functional>
 #include <string>
 #include <vector>
@@ -81,7 +82,8 @@ struct sr_ctx {
     std::vector<sr_ctx*> subs;    // the crop contexts made so far (owned)
     int* box_part = nullptr;      // the fit's per-CTA partials
     int* box_rec = nullptr;       // the fitted box (device)
-    unsigned long long box_steps = 0;  // steps since the upload: the refit cadence
+    unsigned long long box_steps = 0;  // steps since the upload (or the restored step index): the refit cadence
+    float* plane32 = nullptr;          // a W*H f32 staging plane (the rate's f32 form), made on first use
     unsigned long long box_fits = 0;
     // timing
     int timing = 0;  // 0 off; 1 each step's device time (captured steps); 2 per pass (passes launched one by one)
@@ -161,7 +163,7 @@ static void ctx_free(sr_ctx* c) {
     cudaFree(c->src); cudaFree(c->phim); cudaFree(c->gxm); cudaFree(c->gym);
     cudaFree(c->kappa);
     for (sr_ctx* s : c->subs) ctx_free(s);
-    cudaFree(c->box_part); cudaFree(c->box_rec);
+    cudaFree(c->box_part); cudaFree(c->box_rec); cudaFree(c->plane32);
     cudaFree(c->table); cudaFree(c->held); cudaFree(c->src_free); cudaFree(c->phip); cudaFree(c->gxp);
     cudaFree(c->gyp); cudaFree(c->push); cudaFree(c->radx); cudaFree(c->rady); cudaFree(c->rpart); cudaFree(c->rbest); cudaFree(c->ridx); cudaFree(c->rfin);
     if (c->grav_ready) c->grav.destroy();
@@ -674,6 +676,24 @@ static void run_steps(sr_ctx* c, uint32_t steps) {
     }
 }
 
+// The world's buffers made current from the crop (with the active box), written by `write`, then the crop made current
+// from them again: the resume calls write the world and let the box's crop follow.
+template <class F>
+static void write_world(sr_ctx* c, bool with_record, F write) {
+    box_sync(c);
+    write();
+    SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->sub) {
+        crop_in(c, c->sub, c->box, with_record);
+        SR_CUDA_TRY(cudaStreamSynchronize(c->sub->stream));
+    }
+}
+
+static float* staging_plane(sr_ctx* c) {
+    if (!c->plane32) dalloc(&c->plane32, c->n);
+    return c->plane32;
+}
+
 extern "C" {
 
 void sr_config_default(sr_config* c) {
@@ -883,6 +903,73 @@ sr_status sr_upload_opacity(sr_ctx* c, const float* kappa) {
                      sizeof(float), c->sub->stream);
             SR_CUDA_TRY(cudaStreamSynchronize(c->sub->stream));
         }
+    });
+}
+
+sr_status sr_set_clock(sr_ctx* c, uint64_t steps, double sim_time, double dt, double dt_next) {
+    return guarded(c, [&] {
+        SR_REQUIRE(c->uploaded, "sr_set_clock: no state uploaded");
+        SR_REQUIRE(std::isfinite(sim_time) && sim_time >= 0.0, "sr_set_clock: sim_time must be finite and >= 0");
+        SR_REQUIRE(std::isfinite(dt) && dt >= 0.0 && std::isfinite(dt_next) && dt_next > 0.0,
+                   "sr_set_clock: dt must be finite and >= 0, dt_next finite and > 0");
+        SR_REQUIRE(steps <= 0xffffffffull, "sr_set_clock: a step index past the GPU's u32 count");
+        write_world(c, true, [&] {
+            DtRecord rec{};  // the guard's finding cleared (latch.rs:496-510)
+            rec.dt = dt;
+            rec.dt_next = dt_next;
+            rec.sim_time = sim_time;
+            rec.steps = steps;
+            SR_CUDA_TRY(cudaMemcpyAsync(c->rec, &rec, sizeof rec, cudaMemcpyHostToDevice, c->stream));
+        });
+        c->box_steps = steps;  // refits follow the restored step index
+    });
+}
+
+sr_status sr_read_heat_rate(sr_ctx* c, float* rate) {
+    return guarded(c, [&] {
+        SR_REQUIRE(rate, "sr_read_heat_rate: null plane");
+        SR_REQUIRE(c->heat, "sr_read_heat_rate: the context runs no heat pass");
+        box_sync(c);
+        float* d = staging_plane(c);
+        heat_rate_to_f32(c->heat, d, c->stream);
+        SR_CUDA_TRY(cudaMemcpyAsync(rate, d, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+}
+
+sr_status sr_set_heat_rate(sr_ctx* c, const float* rate) {
+    return guarded(c, [&] {
+        SR_REQUIRE(c->heat, "sr_set_heat_rate: the context runs no heat pass");
+        write_world(c, false, [&] {
+            float* d = nullptr;
+            if (rate) {
+                d = staging_plane(c);
+                SR_CUDA_TRY(cudaMemcpyAsync(d, rate, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
+            }
+            heat_rate_from_f32(c->heat, d, c->stream);
+        });
+    });
+}
+
+sr_status sr_read_side_flux(sr_ctx* c, float* fx, float* fy) {
+    return guarded(c, [&] {
+        SR_REQUIRE(fx && fy, "sr_read_side_flux: null plane");
+        SR_REQUIRE(c->radx && c->heat, "sr_read_side_flux: the side flux is reference mode's P5 output (14 channels, heat on)");
+        box_sync(c);
+        SR_CUDA_TRY(cudaMemcpyAsync(fx, c->radx, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+        SR_CUDA_TRY(cudaMemcpyAsync(fy, c->rady, sizeof(float) * c->n, cudaMemcpyDeviceToHost, c->stream));
+        SR_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    });
+}
+
+sr_status sr_set_side_flux(sr_ctx* c, const float* fx, const float* fy) {
+    return guarded(c, [&] {
+        SR_REQUIRE(fx && fy, "sr_set_side_flux: null plane");
+        SR_REQUIRE(c->radx && c->heat, "sr_set_side_flux: the side flux is reference mode's P5 output (14 channels, heat on)");
+        write_world(c, false, [&] {
+            SR_CUDA_TRY(cudaMemcpyAsync(c->radx, fx, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
+            SR_CUDA_TRY(cudaMemcpyAsync(c->rady, fy, sizeof(float) * c->n, cudaMemcpyHostToDevice, c->stream));
+        });
     });
 }
 

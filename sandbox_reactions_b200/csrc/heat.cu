@@ -860,6 +860,16 @@ __global__ void zero_kernel(double* a, size_t n) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) a[i] = 0.0;
 }
 
+__global__ void f64_to_f32_kernel(float* dst, const double* __restrict__ src, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+__global__ void f32_to_f64_kernel(double* dst, const float* __restrict__ src, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+
 // One device scalar set by the host's launch (a value captured at launch time, so no staging buffer is reused).
 __global__ void set_scalar_kernel(double* scal, int slot, double value) {
     if (threadIdx.x == 0 && blockIdx.x == 0) scal[slot] = value;
@@ -1682,6 +1692,22 @@ int heat_collect(HeatSolver* H, Learner* L, const float* U, const float* kappa, 
 }
 
 void heat_reset(HeatSolver* H, cudaStream_t s) { SR_CUDA_TRY(cudaMemsetAsync(H->rate, 0, sizeof(double) * H->n, s)); }
+
+void heat_rate_to_f32(HeatSolver* H, float* dst, cudaStream_t s) {
+    f64_to_f32_kernel<<<H->grid, RED_THREADS, 0, s>>>(dst, H->rate, H->n);
+    sr_note_launch();
+    SR_CUDA_TRY(cudaGetLastError());
+}
+
+void heat_rate_from_f32(HeatSolver* H, const float* src, cudaStream_t s) {
+    if (!src) {
+        heat_reset(H, s);
+        return;
+    }
+    f32_to_f64_kernel<<<H->grid, RED_THREADS, 0, s>>>(H->rate, src, H->n);
+    sr_note_launch();
+    SR_CUDA_TRY(cudaGetLastError());
+}
 
 void heat_set_reference(HeatSolver* H, const HeatRef& R) {
     H->ref = R;

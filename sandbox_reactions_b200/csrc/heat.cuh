@@ -43,6 +43,10 @@ long long heat_capture_step(HeatSolver* hs, float* U, const float* kappa, const 
 void heat_graph_launched(HeatSolver* hs);
 // Forgets the last step's rates (a new state was uploaded).
 void heat_reset(HeatSolver* hs, cudaStream_t s);
+// The last step's rates as f32 into `dst` (W*H floats on the device), or set from `src` (nullptr: zeros): the rate a
+// dump carries (crates/sr-engine/src/step/heat.rs:550-582).
+void heat_rate_to_f32(HeatSolver* hs, float* dst, cudaStream_t s);
+void heat_rate_from_f32(HeatSolver* hs, const float* src, cudaStream_t s);
 void heat_set_precond(HeatSolver* hs, uint32_t precond);
 void heat_set_limits(HeatSolver* hs, uint32_t max_passes, uint32_t max_rounds);
 // The first Newton pass's system of a step of length dt, solved alone (timed on the device); `fallback` gets 1 when

@@ -9,9 +9,8 @@ most 16 objects of x, y, vx, vy, m) and ``resume`` (dt, dt_next, latch_since, bo
 and optionally rate, held, mass_carry) (parse_header, dump.rs:292-360). Every departure is refused with a message naming
 it, as Dump::from_bytes refuses (dump.rs:150-215).
 
-``load_into`` hands a dump to a Step: a reference-mode step (14 channels) takes every plane and the hold's mask; a
-4-channel step takes ``Dump.state4()`` (Σ, Σu, Σv, E). F and the rate are kept in the Dump for the caller (the
-reference-mode P5 that reads them is not part of this build).
+``load_into`` hands a dump to a Step as load_dump does (state, hold's mask, F, P5's rate, clock); ``save_from`` takes
+one from a reference-mode Step as dump_state does, so a run stopped and resumed steps on as it would have.
 """
 from __future__ import annotations
 
@@ -233,15 +232,57 @@ def write(dump: Dump, path) -> None:
 
 
 def load_into(step, dump: Dump) -> None:
-    """Uploads the dump into `step` (a sandbox_reactions_b200.engine.Step of the same world): a 4-channel step takes
-    Σ, Σu, Σv, E; a reference-mode step (14 channels) takes every plane and, when the dump holds one, the hold's mask
-    (the reference's resume: State::upload, then State::upload_held, state.rs:198-279)."""
+    """load_dump (crates/sr-engine/src/dump.rs:368-410) into `step` (a sandbox_reactions_b200.engine.Step of the same
+    world): the state (State::upload), then in reference mode (14 channels) the hold's mask (the dump's, or none held)
+    and F into the side flux the next P4 pushes with, then P5's rate (the dump's, or zeros) when the step runs P5, then
+    the clock (Step::restore: the next step's index, the sim time, Δt_n and Δt_n+1) — a dump at step 0 keeps the
+    upload's own initial reduction, as the reference's restore does. A 4-channel step takes Σ, Σu, Σv, E, the rate and
+    the clock; F has no reader there (its P4 takes no radiation force).
+
+    Refused as load_dump refuses: another world than the step's; a step index past the GPU's u32 count; sinks (this
+    build runs no P3 to keep them); in reference mode F without P5 to read it, and P5 without F (its first step would
+    push with F = 0)."""
     c, h, w = step.shape
     if (h, w) != (dump.height, dump.width):
         raise DumpError(f"dump world {dump.width} x {dump.height}, the step's {w} x {h}")
-    if c == len(CHANNELS):
+    if dump.step > 0xFFFFFFFF:
+        raise DumpError(f"dump step {dump.step}: past the GPU's u32 step count")
+    if dump.sinks:
+        raise DumpError(f"dump holds {len(dump.sinks)} sink(s), and this step runs no P3 to keep them")
+    heat = bool(step.config.heat)
+    ref = c == len(CHANNELS)
+    if ref and dump.flux is not None and not heat:
+        raise DumpError("dump holds F, and this step runs no P5 to keep it (heat off)")
+    if ref and dump.flux is None and heat:
+        raise DumpError("dump holds no F, and this step runs P5: its first step would push with F = 0")
+    if ref:
         step.upload(np.ascontiguousarray(dump.planes, np.float32))
-        if dump.held is not None:
-            step.upload_held(dump.held)
-        return
-    step.upload(dump.state4())
+        held = dump.held if dump.held is not None else np.zeros((h, w), np.uint32)
+        step.upload_held(held)
+        if dump.flux is not None:
+            step.set_side_flux(dump.flux[0], dump.flux[1])
+    else:
+        step.upload(dump.state4())
+    if heat:
+        step.set_heat_rate(dump.rate)
+    if dump.step > 0:
+        step.set_clock(dump.step, dump.sim_time, dump.dt, dump.dt_next)
+
+
+def save_from(step) -> Dump:
+    """dump_state (crates/sr-engine/src/dump.rs:355-366) of a reference-mode step (14 channels): the state, the step
+    index and sim time, Δt_n and Δt_n+1, and with P5 the side flux F and P5's rate; the hold's mask when any cell is
+    held. A 4-channel step is refused: a dump holds the 14 canonical channels, and that step has no species."""
+    c, h, w = step.shape
+    if c != len(CHANNELS):
+        raise DumpError(f"a dump holds the {len(CHANNELS)} canonical channels; this step carries {c} (no species)")
+    planes = step.readback()
+    clock = step.read_dt()
+    held = step.read_held()
+    flux = rate = None
+    if step.config.heat:
+        flux = np.stack(step.read_side_flux())
+        rate = step.read_heat_rate()
+    return Dump(width=w, height=h, step=int(clock.steps), sim_time=float(clock.sim_time), planes=planes,
+                dt=float(clock.dt), dt_next=float(clock.dt_next), flux=flux, rate=rate,
+                held=held.astype(np.uint8) if held.any() else None)

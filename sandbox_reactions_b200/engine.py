@@ -58,6 +58,11 @@ def load_library(path: str = LIB_PATH):
     L.sr_read_heat.argtypes = [P, C.POINTER(sr_heat_report)]
     L.sr_gravity_field.argtypes = [P, F, F, F]
     L.sr_heat_flux.argtypes = [P, F, F]
+    L.sr_set_clock.argtypes = [P, C.c_uint64, C.c_double, C.c_double, C.c_double]
+    L.sr_read_heat_rate.argtypes = [P, F]
+    L.sr_set_heat_rate.argtypes = [P, F]
+    L.sr_read_side_flux.argtypes = [P, F, F]
+    L.sr_set_side_flux.argtypes = [P, F, F]
     L.sr_set_edge_mode.argtypes = [P, C.c_uint32]
     L.sr_set_heat_precond.argtypes = [P, C.c_uint32]
     L.sr_set_heat_limits.argtypes = [P, C.c_uint32, C.c_uint32]
@@ -98,7 +103,8 @@ def load_library(path: str = LIB_PATH):
     for name in ("sr_create", "sr_upload", "sr_readback", "sr_upload_opacity", "sr_upload_held", "sr_read_held", "sr_read_box",
                  "sr_step", "sr_read_dt",
                  "sr_read_heat", "sr_gravity_field", "sr_heat_flux", "sr_set_edge_mode", "sr_set_heat_precond",
-                 "sr_set_heat_limits", "sr_set_timing", "sr_read_cost", "sr_heat_first_solve"):
+                 "sr_set_heat_limits", "sr_set_timing", "sr_read_cost", "sr_heat_first_solve", "sr_set_clock",
+                 "sr_read_heat_rate", "sr_set_heat_rate", "sr_read_side_flux", "sr_set_side_flux"):
         getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -211,6 +217,41 @@ class Step:
         gx, gy, phi = (np.empty((h, w), np.float32) for _ in range(3))
         self._check(self.lib.sr_gravity_field(self._h, _fptr(gx), _fptr(gy), _fptr(phi)))
         return phi, gx, gy
+
+    # ---- the records a dump carries beyond the cells (dump_state / load_dump, dump.rs:355-410)
+    def set_clock(self, steps: int, sim_time: float, dt: float, dt_next: float):
+        """Step::restore (step/latch.rs:493-510): the next step's index, the sim time, Δt_n and the next Δt."""
+        self._check(self.lib.sr_set_clock(self._h, int(steps), float(sim_time), float(dt), float(dt_next)))
+
+    def read_heat_rate(self, out: np.ndarray | None = None) -> np.ndarray:
+        """Step::heat_rate (step/heat.rs:550-565): each cell's P5 rate of the last step, (H, W) f32 (into `out`)."""
+        r = np.empty(self.shape[1:], np.float32) if out is None else out
+        if r.shape != self.shape[1:] or r.dtype != np.float32 or not r.flags.c_contiguous:
+            raise SrError(1, f"rate plane of shape {r.shape} {r.dtype}, expected a contiguous f32 {self.shape[1:]}")
+        self._check(self.lib.sr_read_heat_rate(self._h, _fptr(r)))
+        return r
+
+    def set_heat_rate(self, rate: np.ndarray | None):
+        """Step::set_heat_rate (step/heat.rs:566-582): a dump's rate, or zeros for None."""
+        if rate is None:
+            self._check(self.lib.sr_set_heat_rate(self._h, None))
+            return
+        r = np.ascontiguousarray(rate, dtype=np.float32)
+        if r.shape != self.shape[1:]:
+            raise SrError(1, f"rate plane of shape {r.shape}, expected {self.shape[1:]}")
+        self._check(self.lib.sr_set_heat_rate(self._h, _fptr(r)))
+
+    def read_side_flux(self):
+        """Step::side_flux (step/heat.rs:584-589): the cell-centred F_x, F_y the next P4 pushes with, (H, W) each."""
+        fx, fy = np.empty(self.shape[1:], np.float32), np.empty(self.shape[1:], np.float32)
+        self._check(self.lib.sr_read_side_flux(self._h, _fptr(fx), _fptr(fy)))
+        return fx, fy
+
+    def set_side_flux(self, fx: np.ndarray, fy: np.ndarray):
+        a, b = (np.ascontiguousarray(v, dtype=np.float32) for v in (fx, fy))
+        if a.shape != self.shape[1:] or b.shape != self.shape[1:]:
+            raise SrError(1, f"flux planes of shape {a.shape} / {b.shape}, expected {self.shape[1:]}")
+        self._check(self.lib.sr_set_side_flux(self._h, _fptr(a), _fptr(b)))
 
     def read_heat_flux(self):
         h, w = self.shape[1:]

@@ -117,6 +117,68 @@ def test_the_reference_fixtures_read_and_round_trip():
         same(D.from_bytes(d.to_bytes()), d)
 
 
+class StubStep:
+    """The calls load_into and save_from make, recorded (no GPU): a Step of `channels` planes with or without P5."""
+
+    def __init__(self, w=64, h=64, channels=14, heat=True):
+        from sandbox_reactions_b200.abi import Config
+
+        self.shape = (channels, h, w)
+        self.config = Config(width=w, height=h, channels=channels, heat=heat)
+        self.calls = []
+
+    def __getattr__(self, name):
+        if name.startswith(("upload", "set_")):
+            return lambda *a: self.calls.append((name, a))
+        raise AttributeError(name)
+
+
+def test_load_into_writes_in_load_dumps_order():
+    # dump.rs:397-409: the state, the hold's mask, F, the rate, then the clock
+    d = sample(sinks=0)
+    st = StubStep()
+    D.load_into(st, d)
+    assert [c[0] for c in st.calls] == ["upload", "upload_held", "set_side_flux", "set_heat_rate", "set_clock"]
+    assert np.array_equal(st.calls[0][1][0], d.planes) and np.array_equal(st.calls[1][1][0], d.held)
+    assert np.array_equal(st.calls[2][1][0], d.flux[0]) and np.array_equal(st.calls[2][1][1], d.flux[1])
+    assert np.array_equal(st.calls[3][1][0], d.rate)
+    assert st.calls[4][1] == (d.step, d.sim_time, d.dt, d.dt_next)
+    # none held: a mask of zeros; no rate: zeros (None); step 0: the upload's own reduction, no clock
+    d2 = sample(sinks=0, rate=False, held=False)
+    d2.step = 0
+    st2 = StubStep()
+    D.load_into(st2, d2)
+    assert [c[0] for c in st2.calls] == ["upload", "upload_held", "set_side_flux", "set_heat_rate"]
+    assert not st2.calls[1][1][0].any() and st2.calls[3][1] == (None,)
+    # a 4-channel step: Σ, Σu, Σv, E, the rate, the clock; no mask, no F
+    st4 = StubStep(channels=4)
+    D.load_into(st4, sample(sinks=0))
+    assert [c[0] for c in st4.calls] == ["upload", "set_heat_rate", "set_clock"]
+    assert st4.calls[0][1][0].shape == (4, 64, 64)
+
+
+@pytest.mark.parametrize("case,message", [
+    ("world", "dump world 64 x 64, the step's 72 x 64"),
+    ("step", "past the GPU's u32 step count"),
+    ("sinks", "runs no P3"),
+    ("flux_no_heat", "dump holds F, and this step runs no P5"),
+    ("heat_no_flux", "its first step would push with F = 0"),
+])
+def test_load_into_refuses_what_load_dump_refuses(case, message):
+    d = sample(sinks=1 if case == "sinks" else 0, flux=case != "heat_no_flux")
+    st = StubStep(w=72 if case == "world" else 64, heat=case != "flux_no_heat")
+    if case == "step":
+        d.step = 2 ** 32
+    with pytest.raises(D.DumpError, match=message):
+        D.load_into(st, d)
+    assert st.calls == []  # refused before anything was written
+
+
+def test_save_from_refuses_a_step_without_species():
+    with pytest.raises(D.DumpError, match="no species"):
+        D.save_from(StubStep(channels=4))
+
+
 @pytest.mark.gpu
 def test_a_dumped_state_steps_as_the_state_itself():
     from sandbox_reactions_b200 import scenes
