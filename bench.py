@@ -16,12 +16,13 @@ as one captured graph per batch step against the same worlds one at a time (`bat
 world with every host thread, for as many of the K steps as fit a bounded time (at least one), and beside it one
 thread on a 512² sample of the scene.
 
-`--case fld|full|learned|sod|grav --size S` runs one small self-contained workload per hot kernel family instead (what
+`--case fld|full|learned|sod|grav|ref --size S` runs one small self-contained workload per hot kernel family instead (what
 the committed ncu summaries were captured on) and prints one line with its device time: fld, the implicit-diffusion
 world's first system solved to 1e-8 `--solves` times (smoothers, coarse tail, SpMV, PCG vectors; `--sweeps 4` for
 V(4,4)); full, `--steps` full steps of the benchmark world; learned, one flexible-CG round with an untrained learned
 preconditioner (the convolution kernels' cost does not depend on the weights); sod, `--steps` hydro-only steps of a
-Sod tube (the stencil kernel); grav, `--solves` gravity-only steps of a disk (the FFT kernels).
+Sod tube (the stencil kernel); grav, `--solves` gravity-only steps of a disk (the FFT kernels); ref, `--steps`
+reference-mode steps (14 channels, scenes.ref_disk: the reference-mode P4 kernel).
 """
 from __future__ import annotations
 
@@ -247,6 +248,15 @@ def run_case(args, local):
             ms, _, _, _ = s.heat_first_solve(cfg.dt_fixed, "learned")
             s.attach_learner(None)
         print(f"learned {n}: one round {ms:.3f} ms")
+    elif args.case == "ref":
+        cfg, P = scenes.ref_disk(n)
+        with Step(cfg) as s:
+            s.upload(P)
+            s.set_timing(2)
+            s.run(args.steps)
+            cost = s.read_cost()
+        print(f"ref {n}: {args.steps} reference-mode steps, {cost.total_ms / args.steps:.3f} ms per step, "
+              f"P4 {cost.hydro_ms / args.steps:.3f} ms per step")
     elif args.case == "sod":
         cfg, P = scenes.sod(n)
         with Step(cfg) as s:
@@ -570,7 +580,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=120.0,
                     help="seconds of timed twin steps the reference arm may spend (at least one step)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--case", choices=["fld", "full", "learned", "sod", "grav"],
+    ap.add_argument("--case", choices=["fld", "full", "learned", "sod", "grav", "ref"],
                     help="run one profiling workload instead of the benchmark")
     ap.add_argument("--solves", type=int, default=3)
     ap.add_argument("--precond", default="mg")

@@ -9,10 +9,14 @@ Seeds follow seed = 1000 + 100 * config + scene. Each generator returns (Config,
                 explicit diffusion limit;
   - full_step:  the disk of config 2 with the opacity field of config 3 and hot spots at T = 100 over T = 1 (the
                 reference's burning temperatures are 56-135), every pass on (the
-                hydro+gravity+FLD step of the headline metric).
+                hydro+gravity+FLD step of the headline metric);
+  - ref_disk:   reference mode (14 channels): a scene-JSON world of a warm solar-mix disk with a hot helium core
+                over a thin hydrogen background, laid down with the reference's EOS and species, gravity, hydro and
+                heat on (the radiation force from the second step) — the reference-mode P4 kernel's workload.
 """
 from __future__ import annotations
 
+import json
 import math
 
 import numpy as np
@@ -180,3 +184,24 @@ def batch_mix(count: int = 64, sizes=(256, 512, 1024, 2048), scene: int = 0):
 def world(spec):
     n, scene, mass = spec
     return full_step(n, scene=scene, sigma0=mass)
+
+
+def ref_disk(n: int = 1024):
+    """Reference mode: returns (cfg, planes (14, H, W) f32) of a scene laid down by scene.py at n x n."""
+    from .scene import Scene
+
+    a, core = 0.3125 * n, 0.0625 * n
+    text = json.dumps({
+        "version": 1, "world": {"width": n, "height": n, "edge": "leave"}, "slowdown": False,
+        "switches": {"gravity": True, "hydro": True, "heat": True, "reactions": False, "neutrinos": False,
+                     "sinks": False},
+        "objects": [
+            {"kind": "rect", "x0": 0, "y0": 0, "w": n, "h": n, "sigma": 2e-3, "t": 1.0, "composition": {"H": 1.0},
+             "v": [0, 0]},
+            {"kind": "disk", "x": n / 2, "y": n / 2, "a": a, "sigma_c": 1.0, "t": 40.0,
+             "composition": {"H": 0.7346, "He": 0.2485, "C": 0.0092, "O": 0.0077}, "v": [0.05, 0.02]},
+            {"kind": "disk", "x": 0.41 * n, "y": 0.55 * n, "a": core, "sigma_c": 2.0, "t": 400.0,
+             "composition": {"He": 1.0}, "v": [0, 0]}]})
+    sc = Scene.parse(text)
+    P, _ = sc.planes()
+    return sc.ref_config(strict=False).replace(heat=True), P
