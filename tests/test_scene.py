@@ -291,3 +291,16 @@ def test_every_reference_scene_file_parses_and_lays_down_without_warnings():
     fill = S.Scene.load(os.path.join(REF_SCENES, "fill_world.json"))
     for w, h in ((64, 64), (600, 400), (2048, 64), (64, 2048)):
         assert (fill.planes((w, h))[0][0] > np.float32(1e-8)).all()
+
+
+def test_the_reference_mode_benchmark_world_lays_down_as_a_scene():
+    # scenes.ref_disk (bench.py --case ref): 14 canonical planes, the mass fractions summing to 1 in every cell, the
+    # helium core's mass mixed into the disk's solar mix (objects add their mass: He well above the disk's 0.2485),
+    # reference mode with gravity, hydro and heat on
+    from sandbox_reactions_b200 import scenes
+
+    cfg, P = scenes.ref_disk(128)
+    assert P.shape == (14, 128, 128) and P.dtype == np.float32 and np.isfinite(P).all()
+    assert cfg.channels == 14 and cfg.heat and cfg.gravity and cfg.hydro
+    assert np.abs(P[4:].sum(axis=0) - 1.0).max() < 1e-5
+    assert P[5].max() > 0.5 and P[0].max() > 1.0 and P[0].min() >= 1e-3
